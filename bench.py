@@ -1,0 +1,352 @@
+#!/usr/bin/env python
+"""Benchmark: Kaiser-Bessel NUFFT forward + adjoint throughput on B200.
+
+Workload (one "step"): the 2D multi-coil CG-SENSE geometry -- 256x256
+complex64 coil images (32 coils = Gaussian coil maps x random-ellipse
+phantom), variable-density spiral of 48 interleaves x 2048 samples,
+oversampling 1.25, kernel width 6 (the triton_nufft defaults) -- one forward
+NUFFT of all coils followed by one adjoint NUFFT of all coils. Metric:
+C * M / (t_fwd + t_adj) in Msample*coil/s. Inputs resident in HBM; L2 flushed
+(256 MB write) between timed steps, outside the timed events.
+
+Also reported on the same line: the gridding / interpolation kernel roofline
+(stage times measured live with CUDA events inside the fused calls), the
+end-to-end number through the public API with pinned host buffers, CG-SENSE
+solves/s (20 iterations, lambda 1e-3, graph-captured vs eager), the CPU
+oracle baseline, and SM clocks sampled during the timed region.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU: launched by torchrun, one independent replica per rank (weak
+scaling, no data-path collective), time = max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "NUFFT fwd+adj Msamples·coil/s; batched CG-SENSE solves/s at ≤1e-4 rel err"
+UNIT = "Msample·coil/s"
+IM = (256, 256)
+NCOIL = 32
+NINTL, NSAMP = 48, 2048
+OS, W = 1.25, 6
+WORKLOAD = "2D multi-coil KB NUFFT fwd+adj: 256x256 c64, 32 coils, VD spiral 48x2048, os 1.25, W 6"
+# DRAM traffic per gridding launch from an ncu capture of this workload
+# (profiles/grid_kernel_spiral256_c32.md); None until captured.
+GRID_TRAFFIC_BYTES = None
+INTERP_TRAFFIC_BYTES = None
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def make_inputs(seed):
+    from mr_recon_b200 import synth
+    rng = np.random.RandomState(seed)
+    x = synth.ellipse_phantom(IM, 20, rng)
+    mps = synth.gaussian_coil_maps(IM, NCOIL)
+    imgs = (mps * x[None]).astype(np.complex64)[None]  # (1, C, 256, 256)
+    trj = synth.vd_spiral(NINTL, NSAMP, IM[0] / 2.0)[None]  # (1, 48, 2048, 2)
+    return x, mps, imgs, trj
+
+
+class ClockSampler:
+    """nvidia-smi SM clock / throttle sampling during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [v.strip() for v in line.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(trj, imgs, coils, repeats=1):
+    """The CPU oracle (a numpy restatement of the reference's CPU path) on
+    `coils` coils, one coil per thread. Returns (Msample*coil/s, threads, seconds)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import nufft_oracle as O
+    O.FFT_WORKERS = 1
+    threads = min(coils, os.cpu_count() or 1)
+    nf = O.KBNufftOracle(IM, OS, W)
+    M = trj[0].reshape(-1, 2).shape[0]
+    t_total = 0.0
+    with ThreadPoolExecutor(threads) as ex:
+        for _ in range(repeats):
+            t0 = time.perf_counter()
+            ks = list(ex.map(lambda c: nf.forward(imgs[:, c:c + 1], trj), range(coils)))
+            list(ex.map(lambda c: nf.adjoint(ks[c], trj), range(coils)))
+            t_total += time.perf_counter() - t0
+    return coils * M * repeats / t_total / 1e6, threads, t_total
+
+
+def run_reference(args, rank):
+    """--impl reference: the CPU oracle port of the reference path on the host
+    cores, rank 0 only; each step is a bounded sample (a few coils)."""
+    if rank != 0:
+        return
+    _, _, imgs, trj = make_inputs(0)
+    ncores = os.cpu_count() or 1
+    per = max(1, args.steps + args.warmup)
+    coils = int(max(1, min(ncores, 8, 160 // per)))
+    for _ in range(min(args.warmup, 1)):
+        cpu_baseline(trj, imgs, coils, 1)
+    v, thr, secs = cpu_baseline(trj, imgs, coils, args.steps)
+    M = NINTL * NSAMP
+    ms = secs / args.steps * 1e3
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "complex64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_coils_per_step": coils, "samples_per_coil": M},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": thr, "kind": "port",
+                         "sample": f"{coils} of 32 coils per step, full 98304-sample spiral, fwd+adj"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cg", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from mr_recon_b200.fourier import b200_nufft
+    from mr_recon_b200.linops import sense_linop
+    from mr_recon_b200.algs import SenseCG
+    from mr_recon_b200 import synth
+
+    if args.warmup < 3:
+        args.warmup = 3
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=dev, timeout=__import__("datetime").timedelta(seconds=120))
+
+    x_np, mps_np, imgs_np, trj_np = make_inputs(1234 + rank)
+    imgs = torch.from_numpy(imgs_np).to(dev)
+    trj = torch.from_numpy(trj_np).to(dev)
+    C, M = NCOIL, NINTL * NSAMP
+    nf = b200_nufft(IM, oversamp=OS, width=W)
+    ksp = nf.forward(imgs, trj)
+    back = nf.adjoint(ksp, trj)
+    torch.cuda.synchronize()
+    plan = nf._plans.entries[-1][2]
+    stats = plan.stats()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+
+    def step():
+        k = nf.forward(imgs, trj)
+        nf.adjoint(k, trj)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    plan.enable_timing(True)
+    plan.timing()  # clear
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()
+        evs[i][0].record()
+        step()
+        evs[i][1].record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    stage = plan.timing()
+    plan.enable_timing(False)
+    total_ms = sum(a.elapsed_time(b) for a, b in evs)
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    value = world * C * M * args.steps / (total_ms / 1e3) / 1e6
+
+    # roofline of the dominant kernel (gridding or interpolation)
+    peak, peak_kind = load_peaks()
+    Gos = math.prod(math.ceil(OS * n) for n in IM)
+    alg = 8 * C * Gos + 8 * C * M + 4 * 2 * M
+    g_ms = stage["grid"][0] / max(1, stage["grid"][1])
+    i_ms = stage["interp"][0] / max(1, stage["interp"][1])
+    dom, dms, traffic = ("grid", g_ms, GRID_TRAFFIC_BYTES) if g_ms >= i_ms else ("interp", i_ms, INTERP_TRAFFIC_BYTES)
+    achieved = alg / (dms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                "algorithmic_bytes": alg, "kernel_ms": dms,
+                "stage_ms_per_step": {k: v[0] / args.steps for k, v in stage.items() if v[1]}}
+
+    # end to end through the public API with pinned host buffers
+    img_h = imgs.cpu().pin_memory()
+    ksp_h = torch.empty(ksp.shape, dtype=ksp.dtype).pin_memory()
+    ksp_in_h = ksp.cpu().pin_memory()
+    out_h = torch.empty(back.shape, dtype=back.dtype).pin_memory()
+
+    def e2e_step():
+        a = img_h.to(dev, non_blocking=True)
+        k = nf.forward(a, trj)
+        ksp_h.copy_(k, non_blocking=True)
+        b = ksp_in_h.to(dev, non_blocking=True)
+        o = nf.adjoint(b, trj)
+        out_h.copy_(o, non_blocking=True)
+
+    for _ in range(3):
+        e2e_step()
+    torch.cuda.synchronize()
+    ne = max(5, min(args.steps, 50))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(ne):
+        e2e_step()
+    e1.record()
+    torch.cuda.synchronize()
+    te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_val = world * C * M * ne / (float(te.item()) / 1e3) / 1e6
+    nbytes_img = img_h.numel() * 8
+    nbytes_ksp = ksp_h.numel() * 8
+    e2e = {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": nbytes_img + nbytes_ksp,
+           "d2h_bytes_per_step": nbytes_ksp + nbytes_img, "steps": ne}
+
+    # CG-SENSE solves/s (20 iterations, lambda 1e-3), graph vs eager
+    cg = None
+    if not args.no_cg:
+        rng = np.random.RandomState(99 + rank)
+        A = sense_linop(trj[0], torch.from_numpy(mps_np).to(dev), nufft=nf)
+        kk = A.forward(torch.from_numpy(x_np).to(dev))
+        kk = torch.from_numpy(synth.add_noise(kk.cpu().numpy(), 30.0, rng)).to(dev)
+        max_eig = 1.0
+        for _ in range(15):  # power method (setup, not timed)
+            v = torch.randn(IM, dtype=torch.complex64, device=dev) if _ == 0 else v
+            z = A.normal(v)
+            max_eig = float(torch.linalg.vector_norm(z))
+            v = z / max_eig
+        max_eig *= 1.01
+        solver = SenseCG(A.plan, A.mps, A.dcf, 20, 1e-3, max_eig)
+        solver.ksp.copy_(kk.reshape(-1))
+        x_eager = solver.solve().clone()
+        solver.capture()
+        x_graph = solver.solve().clone()
+        reps = 20
+        torch.cuda.synchronize()
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record()
+        for _ in range(reps):
+            solver.graph.replay()
+        c1.record()
+        torch.cuda.synchronize()
+        g_ms = c0.elapsed_time(c1) / reps
+        solver.graph = None
+        c0.record()
+        for _ in range(5):
+            solver.solve()
+        c1.record()
+        torch.cuda.synchronize()
+        e_ms = c0.elapsed_time(c1) / 5
+        cg = {"solves_per_s_graph": world * 1e3 / g_ms, "solves_per_s_eager": world * 1e3 / e_ms,
+              "ms_per_solve_graph": g_ms, "iterations": 20, "lambda": 1e-3,
+              "graph_vs_eager_rel_diff": float((x_graph - x_eager).norm() / x_eager.norm())}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, thr, secs = cpu_baseline(trj_np, imgs_np, 8, 2)
+        cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port",
+               "sample": "8 of 32 coils (one per thread), full 98304-sample spiral, fwd+adj, 2 repeats",
+               "seconds": secs}
+
+    launches_per_step = 4 + (1 if stats["split_tiles"] > 0 else 0)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "complex64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "coils": C, "samples": M, "grid": [320, 320],
+                       "l2": "flushed between steps (256 MB write, outside the timed events)",
+                       "parallelism": f"replicas x{world}", "plan": stats},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "cg_sense": cg,
+            "gpu_launches": launches_per_step * args.steps, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,183 @@
+/*
+ * mrnufft -- B200 (sm_100a) Kaiser-Bessel NUFFT for MRI reconstruction.
+ *
+ * C ABI of libmrnufft.so. Every pointer argument is DEVICE memory owned by the
+ * caller unless stated otherwise; every call is asynchronous on the given
+ * CUDA stream (a cudaStream_t passed as void*, NULL = legacy default stream)
+ * and returns MRN_OK (0) or a negative MRN_ERR_* code. No C++ exception
+ * crosses this boundary. A plan is not thread-safe: use one plan per stream.
+ *
+ * Data conventions (those of mr_recon's triton_nufft, src/mr_recon/fourier.py):
+ *   complex values  : complex64, interleaved re/im (torch.view_as_real layout)
+ *   image           : slice-major, per slice [C][N0][N1][N2] (last axis fastest)
+ *   k-space samples : per slice [C][M]
+ *   trajectory      : per slice [M][ndim] float32, grid units k_i in [-N_i/2, N_i/2)
+ *   oversampled grid: per slice [C][Nos0][Nos1][Nos2], Nos_i = ceil(os * N_i),
+ *                     centred (DC at index Nos_i//2), as forward_FT_only returns
+ * A "plan" holds n_slices independent NUFFT problems that share ndim, width,
+ * oversampling and beta but may differ in image size, sample count and coil
+ * count (uneven batches); slices are laid out back to back in every buffer,
+ * at the offsets reported by mrn_plan_offsets().
+ */
+#ifndef MRNUFFT_H
+#define MRNUFFT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MRN_OK 0
+#define MRN_ERR_ARG (-1)      /* bad argument: shape, dims, null pointer, layout */
+#define MRN_ERR_WIDTH (-2)    /* kernel width outside [1, 15] (mirrors the ValueError of
+                                 ungrid.py:132-143 get_block_width for too-wide kernels) */
+#define MRN_ERR_CUDA (-3)     /* CUDA runtime error (see mrn_last_cuda_error) */
+#define MRN_ERR_CUFFT (-4)    /* cuFFT error */
+#define MRN_ERR_NOMEM (-5)    /* device allocation failed */
+#define MRN_ERR_STATE (-6)    /* plan used before mrn_plan_set_traj */
+#define MRN_ERR_UNSUPPORTED (-7)
+
+/* Plan flags */
+#define MRN_PLAN_RAW 1        /* im_size is the grid size itself; trajectories are grid
+                                 coordinates used as-is (reference ungrid/grid,
+                                 triton_interp/ungrid.py:34, grid.py:32); no FFT stage */
+#define MRN_PLAN_NO_APOD 2    /* apodize=False (fourier.py:366) */
+
+typedef struct mrn_plan mrn_plan;
+
+const char* mrn_version(void);
+const char* mrn_error_string(int code);
+int mrn_last_cuda_error(void);
+
+/*
+ * Create a plan. Replaces triton_nufft.__init__ (fourier.py:361-374) plus the
+ * per-call shape preparation of prep_ungrid_shapes / prep_grid_shapes
+ * (ungrid.py:851-894, grid.py:508-553), hoisted to once per geometry.
+ *   ndim       1, 2 or 3
+ *   im_size    [n_slices * ndim] image size per slice (grid size with MRN_PLAN_RAW)
+ *   n_pts      [n_slices] samples per slice
+ *   n_coil     [n_slices] image batch (coils) per slice
+ *   width      kernel width per dimension, [ndim] (reference `width` tuple)
+ *   beta       KB shape parameter; beta <= 0 selects the reference default
+ *              pi*sqrt((W/os*(os-0.5))^2 - 0.8) of fourier.py:372
+ *   tile       [ndim] tile edge in grid cells, or NULL for the built-in choice
+ *   coil_group coils per CTA, 0 = built-in choice
+ *   max_chunk  maximum samples per work item, 0 = built-in choice
+ * Host arrays: im_size, n_pts, n_coil, width, tile. Allocates device memory.
+ */
+int mrn_plan_create(mrn_plan** plan, int ndim, int n_slices, const int* im_size,
+                    const int64_t* n_pts, const int* n_coil, double oversamp,
+                    const double* width, double beta, int flags, const int* tile,
+                    int coil_group, int max_chunk, int device);
+int mrn_plan_destroy(mrn_plan* plan);
+
+/* Host-side layout query: writes n_slices entries to each non-NULL array
+ * (element offsets, in complex64 units for img/ksp/grid, float units for trj). */
+int mrn_plan_offsets(const mrn_plan* plan, int64_t* img_off, int64_t* ksp_off,
+                     int64_t* grid_off, int64_t* trj_off);
+/* Totals: [0] image elems, [1] ksp elems, [2] grid elems, [3] trj floats,
+ * [4] number of tiles, [5] oversampled size dim0, [6] dim1, [7] dim2 (slice 0). */
+int mrn_plan_sizes(const mrn_plan* plan, int64_t* out8);
+/* Host-side, after a synchronize: number of interp and gridding work items,
+ * gridding entries, and split (multi-item) gridding tiles, in out4. */
+int mrn_plan_stats(mrn_plan* plan, int64_t* out4);
+
+/* Stage timing, a profiling aid with no counterpart in the reference (which
+ * only prints wall-clock, recons.py:127-133). When on, every call records a
+ * CUDA event pair around each stage on the launching stream (not for use
+ * under stream capture). mrn_plan_timing waits for the recorded events,
+ * writes per-stage total milliseconds and counts for the 8 stages
+ *   0 pre-FFT  1 FFT  2 interpolation  3 gridding  4 post-iFFT
+ *   5 layout copy  6 trajectory gradient  7 CG vector ops
+ * and clears the record. */
+int mrn_plan_enable_timing(mrn_plan* plan, int on);
+int mrn_plan_timing(mrn_plan* plan, double* ms8, int64_t* count8);
+
+/*
+ * Bind a trajectory (device, float32, all slices back to back). Scales it
+ * (triton_nufft._scale_trj, fourier.py:420-430), wraps it circularly
+ * (torch.remainder, ungrid.py:873), and sorts the samples into spatial tiles
+ * for both interpolation and gridding. Asynchronous; safe to capture in a
+ * CUDA graph. Must be called again when the trajectory values change.
+ */
+int mrn_plan_set_traj(mrn_plan* plan, const float* trj, void* stream);
+
+/* Full NUFFT. forward: triton_nufft.forward = forward_interp_only(forward_FT_only)
+ * (fourier.py:230-252, 432-503). adjoint: adjoint_iFT_only(adjoint_grid_only)
+ * (fourier.py:254-276, 505-550). img/ksp in the slice layout above. */
+int mrn_forward(mrn_plan* plan, const void* img, void* ksp, void* stream);
+int mrn_adjoint(mrn_plan* plan, const void* ksp, void* img, void* stream);
+
+/* Split stages with the reference's centred grid layout.
+ * forward_ft  : triton_nufft.forward_FT_only   (fourier.py:432-468)
+ * interp      : triton_nufft.forward_interp_only (fourier.py:470-503), output * scale
+ * grid        : triton_nufft.adjoint_grid_only (fourier.py:527-550), output * scale
+ * adjoint_ift : triton_nufft.adjoint_iFT_only  (fourier.py:505-525)
+ * With MRN_PLAN_RAW, interp/grid are ungrid/grid of triton_interp (ungrid.py:34,
+ * grid.py:32) with pad_mode='circular', norm='1', kernel='kaiser_bessel'. */
+int mrn_forward_ft(mrn_plan* plan, const void* img, void* grid, void* stream);
+int mrn_interp(mrn_plan* plan, const void* grid, void* ksp, float scale, void* stream);
+int mrn_grid(mrn_plan* plan, const void* ksp, void* grid, float scale, void* stream);
+int mrn_adjoint_ift(mrn_plan* plan, const void* grid, void* img, void* stream);
+
+/*
+ * Trajectory gradient (no counterpart in the reference: InterpolateFn.backward,
+ * triton_interp/interp.py:51-74, returns grad_locs=None). For the centred grid
+ * G (as mrn_forward_ft writes) and sample weights S (both complex64), writes
+ * grad[p, i] = scale * Re sum_c conj(S[c,p]) * sum_j dW(u_p - j)/du_i * G[c,j]
+ * times d u_i / d k_i, i.e. the derivative of Re<S, interp(G)> w.r.t. the
+ * trajectory k (float32, slice layout [M][ndim]).
+ */
+int mrn_traj_grad(mrn_plan* plan, const void* grid, const void* samples, float* grad,
+                  float scale, void* stream);
+
+/*
+ * SENSE operator of sense_linop (linops.py:1041-1308) with identity
+ * spatial/temporal functions, one image per slice:
+ *   forward: ksp[c] = NUFFT(mps[c] * x)                   (linops.py:1134-1178)
+ *   adjoint: x = sum_c conj(mps[c]) NUFFT^H(dcf * ksp[c])  (linops.py:1180-1228)
+ *   normal : out = adjoint(forward(x)) * out_scale + lam * x (linops.py:1230-1247)
+ * x/out: per slice [N...]; mps: per slice [C][N...] (image layout); dcf: per
+ * slice [M] float32 or NULL. With pap != NULL, normal also accumulates
+ * Re<x, out> per slice into pap[slice * pap_stride] (float64, caller zeroes
+ * it; pass the CG state + 1 with stride 8 to feed mrn_cg_step directly).
+ */
+int mrn_sense_forward(mrn_plan* plan, const void* x, const void* mps, void* ksp, void* stream);
+int mrn_sense_adjoint(mrn_plan* plan, const void* ksp, const float* dcf, const void* mps,
+                      void* x, float out_scale, void* stream);
+int mrn_sense_normal(mrn_plan* plan, const void* x, const void* mps, const float* dcf,
+                     void* out, float out_scale, float lam, double* pap, int pap_stride,
+                     void* stream);
+
+/*
+ * Conjugate-gradient vector steps for n_slices independent systems (the loop
+ * body of conjugate_gradient, algs.py:779-872), complex64 vectors with
+ * float64 dot products and norms; per-slice scalars stay on the device, so a
+ * whole solve can be captured in a CUDA graph. Vectors use the per-slice
+ * image layout (one image per slice). state: float64 [n_slices * 8] owned by
+ * the caller:
+ *   [0] rz  [1] pAp (accumulated)  [2] rr (accumulated)  [3] done  [4] tol^2
+ *   [5] iterations  [6] last alpha  [7] last beta
+ * mrn_cg_init : zero state; r = b - Ab (Ab given), p = r, x = b, rz = |r|^2
+ * per iteration: Ap = (A^H A + lam) p accumulating pAp into state[1]
+ *                (mrn_sense_normal with pap = state + 1, pap_stride = 8), then
+ * mrn_cg_step : alpha = rz/pAp; x += alpha p; r -= alpha Ap; rr = |r|^2
+ * mrn_cg_dir  : done |= rr < tol^2; beta = rr/rz; p = r + beta p; rz = rr;
+ *               pAp = rr = 0 for the next iteration
+ * Once a slice is done its vectors are left unchanged (the reference breaks
+ * out of the loop at the same point, algs.py:859-860).
+ */
+int mrn_cg_init(mrn_plan* plan, const void* b, const void* Ab, void* x, void* r, void* p,
+                double* state, double tol, void* stream);
+int mrn_cg_step(mrn_plan* plan, void* x, void* r, const void* p, const void* Ap,
+                double* state, void* stream);
+int mrn_cg_dir(mrn_plan* plan, const void* r, void* p, double* state, void* stream);
+/* Per-slice Re<a, b> in float64, accumulated into out[slice] (caller zeroes). */
+int mrn_cg_dot(mrn_plan* plan, const void* a, const void* b, double* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MRNUFFT_H */

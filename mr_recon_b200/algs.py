@@ -1,0 +1,219 @@
+"""Iterative algorithms with the interface of mr_recon's algs.py.
+
+``conjugate_gradient`` (algs.py:779-872), ``power_method_operator``
+(algs.py:364-400), ``FISTA`` (algs.py:655-729) and ``gradient_descent``
+(algs.py:731-777) keep the reference signatures and iteration semantics. Dot
+products and norms are accumulated in float64 and the CG scalars stay on the
+device: the reference's per-iteration ``.item()`` host sync (algs.py:845) and
+early ``break`` become a device-side "done" mask that freezes the iterate at
+the same point, so results match while the loop never waits on the host.
+
+``SenseCG`` is the fused device CG for a ``sense_linop`` on the B200 NUFFT:
+every step is a kernel of libmrnufft.so and a whole solve can be captured in
+one CUDA graph.
+"""
+
+from __future__ import annotations
+
+from typing import Callable, Optional, Tuple
+
+import torch
+from tqdm import tqdm
+
+complex_dtype = torch.complex64
+
+__all__ = ["conjugate_gradient", "power_method_operator", "FISTA", "gradient_descent", "SenseCG"]
+
+
+def _rdot(a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
+    """Re <a, b> = Re sum conj(a) b, accumulated in float64 (0-dim device tensor)."""
+    ar = torch.view_as_real(a.to(complex_dtype).contiguous()).to(torch.float64)
+    br = torch.view_as_real(b.to(complex_dtype).contiguous()).to(torch.float64)
+    return (ar * br).sum()
+
+
+def conjugate_gradient(AHA: Callable, AHb: torch.Tensor, P: Optional[Callable] = None,
+                       num_iters: Optional[int] = 10, lamda_l2: Optional[float] = 0.0,
+                       tolerance: Optional[float] = 1e-8, return_resids: Optional[bool] = False,
+                       weights: Optional[torch.Tensor] = None, verbose=True) -> torch.Tensor:
+    """Complex CG for (AHA + lamda_l2 I) x = AHb starting at x0 = AHb."""
+    if P is None:
+        P = lambda x: x  # noqa: E731
+    if weights is not None:
+        op = lambda x: AHA(x) + lamda_l2 * weights * x  # noqa: E731
+    else:
+        op = lambda x: AHA(x) + lamda_l2 * x  # noqa: E731
+    x0 = AHb.clone()
+    if num_iters == 0:
+        return x0
+    r = AHb - op(x0)
+    z = P(r)
+    p = z.clone()
+    done = torch.zeros((), dtype=torch.bool, device=AHb.device)
+    if return_resids:
+        resids = []
+        xs = [x0.clone()]
+    for _ in tqdm(range(num_iters), "CG Iterations", disable=not verbose):
+        Ap = op(p)
+        pAp = _rdot(p, Ap)
+        rz = _rdot(r, z)
+        alpha = torch.where(done, torch.zeros_like(rz), rz / pAp).to(torch.float32)
+        x0 = x0 + alpha * p
+        r = r - alpha * Ap
+        rr = _rdot(r, r)
+        rnrm = rr.sqrt()
+        if return_resids:
+            resids.append(rnrm.item())
+            xs.append(x0.clone())
+        done = done | (rnrm < tolerance)
+        z = P(r)
+        beta = torch.where(done, torch.zeros_like(rz), _rdot(r, z) / rz).to(torch.float32)
+        p = torch.where(done, p, z + beta * p)
+    if return_resids:
+        return resids, xs
+    return x0
+
+
+def power_method_operator(A: Callable, x0: torch.Tensor, num_iter: Optional[int] = 15,
+                          verbose: Optional[bool] = True) -> Tuple[torch.Tensor, float]:
+    """Largest eigenvalue of A by the power method (algs.py:364-400)."""
+    ll = None
+    for _ in tqdm(range(num_iter), "Max Eigenvalue", disable=not verbose):
+        z = A(x0)
+        ll = torch.linalg.vector_norm(z.to(torch.complex128))
+        x0 = (z / ll).to(z.dtype)
+    if verbose:
+        print(f"Max Eigenvalue = {ll}")
+    return x0, ll.item()
+
+
+def FISTA(AHA: Callable, AHb: torch.Tensor, proxg: Callable, num_iters: Optional[int] = 20,
+          ptol_exit: Optional[float] = 0.5, return_ptols: Optional[bool] = False,
+          return_xs: Optional[bool] = False, x0: Optional[torch.Tensor] = None,
+          verbose: Optional[bool] = True) -> torch.Tensor:
+    """FISTA for ||Ax - b||^2 + g(x) (algs.py:655-729)."""
+    x = AHb.clone() if x0 is None else x0
+    z = x.clone()
+    if num_iters <= 0:
+        return x
+    ptols = []
+    xs = []
+    for k in tqdm(range(num_iters), "FISTA Iterations", disable=not verbose):
+        x_old = x.clone()
+        x = z.clone()
+        gr = AHA(x) - AHb
+        x = proxg(x - gr)
+        if k == 0:
+            z = x
+        else:
+            step = k / (k + 3)
+            z = x + step * (x - x_old)
+        ptol = 100 * torch.linalg.vector_norm(x_old - x) / torch.linalg.vector_norm(x)
+        ptols.append(ptol.item())
+        if ptol < ptol_exit:
+            if verbose:
+                print(f"Tolerance reached after {k + 1} iterations, exiting FISTA")
+            break
+        if return_xs:
+            xs.append(x.clone())
+    if return_ptols:
+        return ptols, x
+    if return_xs:
+        return xs, x
+    return x
+
+
+def gradient_descent(AHA: Callable, AHb: torch.Tensor, lr: float, num_iters: Optional[int] = 100,
+                     lamda_l2: Optional[float] = 0.0, tolerance: Optional[float] = 1e-8,
+                     return_resids: Optional[bool] = False, verbose: Optional[bool] = True):
+    """Gradient descent on (AHA + lamda_l2 I) x = AHb (algs.py:731-777)."""
+    x = AHb
+    op = lambda v: AHA(v) + lamda_l2 * v  # noqa: E731
+    resids = []
+    for _ in tqdm(range(num_iters), "GD Iterations", disable=not verbose):
+        grad = op(x) - AHb
+        x = x - lr * grad
+        nrm = torch.linalg.vector_norm(grad)
+        resids.append(nrm.item())
+        if nrm < tolerance:
+            break
+    if return_resids:
+        return resids, x
+    return x
+
+
+class SenseCG:
+    """CG-SENSE (recons.py:77-156 with max_eigen given) on a fused plan: one
+    image per slice, every slice of the plan solved at once. All scalars stay
+    on the device (float64 state per slice), so ``capture()`` can record the
+    whole solve -- AHb, initial residual and ``max_iter`` iterations -- in one
+    CUDA graph, replayed by ``solve``.
+
+    plan     : mr_recon_b200.plan.Plan with the trajectory bound
+    mps      : coil maps, plan image layout (all slices back to back)
+    dcf      : float32 [total samples] or None
+    """
+
+    def __init__(self, plan, mps: torch.Tensor, dcf: Optional[torch.Tensor], max_iter: int,
+                 lamda_l2: float, max_eigen, tolerance: float = 1e-8):
+        self.plan = plan
+        self.mps = mps
+        self.dcf = dcf
+        self.max_iter = int(max_iter)
+        self.lam = float(lamda_l2)
+        n = plan.nslices
+        dev = plan.device
+        me = torch.as_tensor(max_eigen, dtype=torch.float64).reshape(-1)
+        if me.numel() != 1:
+            raise ValueError("SenseCG takes one max_eigen for all slices")
+        self.max_eigen = float(me[0])
+        self.tol = float(tolerance)
+        nx = sum(int(torch.tensor(s).prod()) for s in plan.im_sizes)
+        mk = lambda: torch.zeros(nx, dtype=complex_dtype, device=dev)  # noqa: E731
+        self.b, self.x, self.r, self.p, self.Ap = mk(), mk(), mk(), mk(), mk()
+        self.state = torch.zeros(n * 8, dtype=torch.float64, device=dev)
+        self.ksp = torch.zeros(plan.n_ksp, dtype=complex_dtype, device=dev)
+        self.graph = None
+
+    def _run(self):
+        pl = self.plan
+        s_adj = 1.0 / self.max_eigen ** 0.5
+        s_nrm = 1.0 / self.max_eigen
+        pl.sense_adjoint(self.ksp, self.dcf, self.mps, self.b, s_adj)
+        if self.max_iter == 0:
+            self.x.copy_(self.b)
+            return
+        pl.sense_normal(self.b, self.mps, self.dcf, self.Ap, s_nrm, self.lam)
+        pl.cg_init(self.b, self.Ap, self.x, self.r, self.p, self.state, self.tol)
+        pap = self.state[1:]
+        for _ in range(self.max_iter):
+            pl.sense_normal(self.p, self.mps, self.dcf, self.Ap, s_nrm, self.lam, pap, 8)
+            pl.cg_step(self.x, self.r, self.p, self.Ap, self.state)
+            pl.cg_dir(self.r, self.p, self.state)
+
+    def capture(self):
+        """Record one full solve in a CUDA graph (after a warm-up run)."""
+        s = torch.cuda.Stream(self.plan.device)
+        s.wait_stream(torch.cuda.current_stream(self.plan.device))
+        with torch.cuda.stream(s):
+            self._run()
+        torch.cuda.current_stream(self.plan.device).wait_stream(s)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self._run()
+        self.graph = g
+        return self
+
+    def solve(self, ksp: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """Run one solve on ``ksp`` (plan k-space layout); returns x (a view
+        of an internal buffer, overwritten by the next solve)."""
+        if ksp is not None:
+            self.ksp.copy_(ksp.reshape(-1))
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            self._run()
+        return self.x
+
+    def iterations(self) -> torch.Tensor:
+        return self.state.view(-1, 8)[:, 5]

@@ -1,0 +1,188 @@
+// Conjugate-gradient vector steps for a batch of independent systems, one
+// image per slice (the loop body of conjugate_gradient, algs.py:779-872).
+// Vectors are complex64; every dot product and norm is accumulated in float64
+// and the per-slice scalars never leave the device, so a solve can be
+// captured in a CUDA graph (the reference calls .item() every iteration,
+// algs.py:845). State per slice, float64[8]:
+//   [0] rz   [1] pAp (accumulated)   [2] rr (accumulated)   [3] done
+//   [4] tol^2   [5] iterations done   [6] alpha   [7] beta
+#include <algorithm>
+
+#include "common.cuh"
+#include "internal.cuh"
+
+namespace mrn {
+
+constexpr int kCgThreads = 256;
+
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x < kCgThreads / 32) t = red[threadIdx.x];
+  if (w == 0)
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  return t;  // valid in thread 0
+}
+
+// r = b - Ab; p = r; x = b; state[0] += |r|^2; state[4] = tol^2
+__global__ void __launch_bounds__(kCgThreads)
+k_cg_init(const SliceGeom* __restrict__ sl, const float2* __restrict__ b, const float2* __restrict__ Ab,
+          float2* __restrict__ x, float2* __restrict__ r, float2* __restrict__ p,
+          double* __restrict__ state, double tol2) {
+  __shared__ double red[kCgThreads / 32];
+  const int s = blockIdx.y;
+  const SliceGeom& g = sl[s];
+  double acc = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < g.nimg;
+       i += (int64_t)gridDim.x * kCgThreads) {
+    const int64_t k = g.x_off + i;
+    const float2 bb = b[k], ab = Ab[k];
+    const float2 rr = make_float2(bb.x - ab.x, bb.y - ab.y);
+    r[k] = rr;
+    p[k] = rr;
+    x[k] = bb;
+    acc += (double)rr.x * rr.x + (double)rr.y * rr.y;
+  }
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) {
+    atomicAdd(state + s * 8 + 0, acc);
+    if (blockIdx.x == 0) state[s * 8 + 4] = tol2;
+  }
+}
+
+// alpha = rz / pAp; x += alpha p; r -= alpha Ap; state[2] += |r|^2 (skipped when done)
+__global__ void __launch_bounds__(kCgThreads)
+k_cg_step(const SliceGeom* __restrict__ sl, float2* __restrict__ x, float2* __restrict__ r,
+          const float2* __restrict__ p, const float2* __restrict__ Ap, double* __restrict__ state) {
+  __shared__ double red[kCgThreads / 32];
+  const int s = blockIdx.y;
+  const SliceGeom& g = sl[s];
+  const double* S = state + s * 8;
+  if (S[3] != 0.0) return;
+  const float alpha = (float)(S[0] / S[1]);
+  double acc = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < g.nimg;
+       i += (int64_t)gridDim.x * kCgThreads) {
+    const int64_t k = g.x_off + i;
+    const float2 pp = p[k], ap = Ap[k];
+    float2 xx = x[k], rr = r[k];
+    xx.x = fmaf(alpha, pp.x, xx.x);
+    xx.y = fmaf(alpha, pp.y, xx.y);
+    rr.x = fmaf(-alpha, ap.x, rr.x);
+    rr.y = fmaf(-alpha, ap.y, rr.y);
+    x[k] = xx;
+    r[k] = rr;
+    acc += (double)rr.x * rr.x + (double)rr.y * rr.y;
+  }
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) atomicAdd(state + s * 8 + 2, acc);
+}
+
+// done |= rr < tol^2; beta = rr / rz; p = r + beta p; then (last block) rz = rr,
+// pAp = rr = 0, iterations += 1.
+__global__ void __launch_bounds__(kCgThreads)
+k_cg_dir(const SliceGeom* __restrict__ sl, int ns, const float2* __restrict__ r,
+         float2* __restrict__ p, double* __restrict__ state, unsigned* __restrict__ counter) {
+  __shared__ bool last;
+  const int s = blockIdx.y;
+  const SliceGeom& g = sl[s];
+  double* S = state + s * 8;
+  const bool done = S[3] != 0.0 || S[2] < S[4];
+  if (!done) {
+    const float beta = (float)(S[2] / S[0]);
+    for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < g.nimg;
+         i += (int64_t)gridDim.x * kCgThreads) {
+      const int64_t k = g.x_off + i;
+      const float2 rr = r[k];
+      float2 pp = p[k];
+      pp.x = fmaf(beta, pp.x, rr.x);
+      pp.y = fmaf(beta, pp.y, rr.y);
+      p[k] = pp;
+    }
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned total = gridDim.x * gridDim.y;
+    last = atomicAdd(counter, 1u) == total - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int q = threadIdx.x; q < ns; q += kCgThreads) {
+    double* T = state + q * 8;
+    if (T[3] == 0.0) {
+      T[6] = T[0] / T[1];
+      if (T[2] < T[4]) {
+        T[3] = 1.0;
+      } else {
+        T[7] = T[2] / T[0];
+        T[0] = T[2];
+      }
+      T[5] += 1.0;
+    }
+    T[1] = 0.0;
+    T[2] = 0.0;
+  }
+  if (threadIdx.x == 0) *counter = 0u;
+}
+
+// out[slice] += Re<a, b> = sum Re(conj(a) b)
+__global__ void __launch_bounds__(kCgThreads)
+k_cg_dot(const SliceGeom* __restrict__ sl, const float2* __restrict__ a, const float2* __restrict__ b,
+         double* __restrict__ out) {
+  __shared__ double red[kCgThreads / 32];
+  const int s = blockIdx.y;
+  const SliceGeom& g = sl[s];
+  double acc = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < g.nimg;
+       i += (int64_t)gridDim.x * kCgThreads) {
+    const int64_t k = g.x_off + i;
+    const float2 aa = a[k], bb = b[k];
+    acc += (double)aa.x * bb.x + (double)aa.y * bb.y;
+  }
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) atomicAdd(out + s, acc);
+}
+
+static dim3 cg_grid(const mrn_plan* P) {
+  int64_t mx = 1;
+  for (const auto& g : P->h_slices) mx = std::max<int64_t>(mx, g.nimg);
+  int64_t bx = (mx + kCgThreads * 4 - 1) / (kCgThreads * 4);
+  bx = std::min<int64_t>(std::max<int64_t>(bx, 1), 1024);
+  return dim3((unsigned)bx, (unsigned)P->nslices);
+}
+
+int launch_cg_init(mrn_plan* P, const float2* b, const float2* Ab, float2* x, float2* r, float2* p,
+                   double* state, double tol, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(state, 0, (size_t)P->nslices * 8 * sizeof(double), st);
+  if (e != cudaSuccess) return cuda_fail(e);
+  k_cg_init<<<cg_grid(P), kCgThreads, 0, st>>>(P->d_slices, b, Ab, x, r, p, state, tol * tol);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? MRN_OK : cuda_fail(e);
+}
+
+int launch_cg_step(mrn_plan* P, float2* x, float2* r, const float2* p, const float2* Ap,
+                   double* state, cudaStream_t st) {
+  k_cg_step<<<cg_grid(P), kCgThreads, 0, st>>>(P->d_slices, x, r, p, Ap, state);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? MRN_OK : cuda_fail(e);
+}
+
+int launch_cg_dir(mrn_plan* P, const float2* r, float2* p, double* state, cudaStream_t st) {
+  k_cg_dir<<<cg_grid(P), kCgThreads, 0, st>>>(P->d_slices, P->nslices, r, p, state, P->d_sync);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? MRN_OK : cuda_fail(e);
+}
+
+int launch_cg_dot(mrn_plan* P, const float2* a, const float2* b, double* out, cudaStream_t st) {
+  k_cg_dot<<<cg_grid(P), kCgThreads, 0, st>>>(P->d_slices, a, b, out);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? MRN_OK : cuda_fail(e);
+}
+
+}  // namespace mrn

@@ -1,0 +1,233 @@
+// Internal declarations shared by the mrnufft CUDA sources (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "../../include/mrnufft.h"
+
+namespace mrn {
+
+constexpr int kMaxDim = 3;
+constexpr int kMaxTaps = 16;     // candidate taps per dim: floor(W) + 1 <= 16 -> W < 16
+constexpr int kThreads = 256;    // threads per CTA of the tile kernels
+constexpr int kWarps = kThreads / 32;
+
+// Geometry of one slice (one NUFFT problem) of a plan. Device-resident table.
+struct SliceGeom {
+  int n[kMaxDim];      // image size (1 for unused dims)
+  int nos[kMaxDim];    // oversampled grid size (grid size for raw plans)
+  int ntile[kMaxDim];  // tiles per dim
+  int hshift[kMaxDim]; // Nos//2: centred index j lives at storage (j - hshift) mod Nos
+  int tile_base;       // first global tile id of this slice
+  int ncoil;           // image batch (coils)
+  int64_t m;           // samples
+  int64_t pt_off;      // first global point id (offset into concatenated points)
+  int64_t img_off;     // complex offset of the slice image block [C][N...]
+  int64_t ksp_off;     // complex offset of the slice samples [C][M]
+  int64_t grid_off;    // complex offset in the plan's internal grid buffer
+  int64_t ugrid_off;   // complex offset in a caller grid buffer (slice order)
+  int64_t x_off;       // complex offset of a one-image-per-slice vector [N...]
+  int64_t gos;         // prod(nos)
+  int64_t nimg;        // prod(n)
+  float scale[kMaxDim];  // trajectory scale ceil(os N)/N (1 for raw)
+  float shift[kMaxDim];  // trajectory shift ceil(os N)//2 (0 for raw)
+  int apod_off[kMaxDim]; // offset of this slice's apodization table per dim
+  int64_t prow_off;      // first grid row (all dims but the last, all coils) of the slice
+  int64_t irow_off;      // first image row (all coils) of the slice
+  int64_t xrow_off;      // first image row of the one-image-per-slice layout
+  float inv_sqrt_n;      // 1 / sqrt(prod(n)) (fourier.py:462, 522)
+};
+
+// Work item: one tile (or a chunk of a heavy tile) of one slice.
+struct Item {
+  int slice;
+  int tile;      // tile id local to the slice
+  int start;     // first entry in the sorted arrays
+  int count;     // entries in this item
+  int split;     // 1 if the tile is shared by several items (gridding: atomic write-back)
+  int pad[3];
+};
+
+struct KBParams {
+  float radius[kMaxDim];  // W_i / 2
+  float beta;
+  int ntaps[kMaxDim];     // candidate taps floor(W_i) + 1
+};
+
+// --------------------------------------------------------------------------
+// Kaiser-Bessel kernel value I0(beta sqrt(1 - x^2)), x = |distance| / radius,
+// the unnormalised kernel of mr_recon (triton_interp/kernels.py:180-246).
+// I0 is evaluated with the polynomial approximations 9.8.1 (z < 3.75) and
+// 9.8.2 (z >= 3.75) of Abramowitz & Stegun, Handbook of Mathematical
+// Functions, p.378 -- the same published approximation the reference uses.
+// --------------------------------------------------------------------------
+__device__ __forceinline__ float as_i0(float z) {
+  if (z < 3.75f) {
+    const float t = z * (1.0f / 3.75f);
+    const float y = t * t;
+    return 1.0f + y * (3.5156229f + y * (3.0899424f + y * (1.2067492f +
+                  y * (0.2659732f + y * (0.0360768f + y * 0.0045813f)))));
+  }
+  const float s = 3.75f / z;
+  const float p = 0.39894228f + s * (0.01328592f + s * (0.00225319f + s * (-0.00157565f +
+                  s * (0.00916281f + s * (-0.02057706f + s * (0.02635537f +
+                  s * (-0.01647633f + s * 0.00392377f)))))));
+  return expf(z) * rsqrtf(z) * p;
+}
+
+// (d/dz as_i0(z)) / z, finite at z = 0 (the small-argument polynomial is even).
+__device__ __forceinline__ float as_di0_over_z(float z) {
+  if (z < 3.75f) {
+    const float t = z * (1.0f / 3.75f);
+    const float y = t * t;
+    const float d = 2.0f * 3.5156229f + y * (4.0f * 3.0899424f + y * (6.0f * 1.2067492f +
+                    y * (8.0f * 0.2659732f + y * (10.0f * 0.0360768f + y * (12.0f * 0.0045813f)))));
+    return d * (1.0f / (3.75f * 3.75f));
+  }
+  const float s = 3.75f / z;
+  const float p = 0.39894228f + s * (0.01328592f + s * (0.00225319f + s * (-0.00157565f +
+                  s * (0.00916281f + s * (-0.02057706f + s * (0.02635537f +
+                  s * (-0.01647633f + s * 0.00392377f)))))));
+  const float dp = 0.01328592f + s * (2.0f * 0.00225319f + s * (3.0f * -0.00157565f +
+                   s * (4.0f * 0.00916281f + s * (5.0f * -0.02057706f + s * (6.0f * 0.02635537f +
+                   s * (7.0f * -0.01647633f + s * (8.0f * 0.00392377f)))))));
+  const float e = expf(z) * rsqrtf(z);
+  const float inv = 1.0f / z;
+  // d/dz [e^z z^-1/2 p(3.75/z)] = e^z z^-1/2 (p - p/(2z) - p'(s) * 3.75/z^2)
+  const float dz = e * (p - 0.5f * p * inv - dp * s * inv);
+  return dz * inv;
+}
+
+// Weight of one tap: dx = (float)j - u in float32, valid iff |dx| <= r
+// (the mask of weights1d..3d, kernels.py:268-393).
+__device__ __forceinline__ float kb_tap(float adx, float r, float beta) {
+  const float x = adx / r;
+  return as_i0(beta * sqrtf(1.0f - x * x));
+}
+
+// d weight / d u for one tap (u the sample coordinate): KB'(x) * sign(u - j) / r.
+__device__ __forceinline__ float kb_tap_du(float dx, float r, float beta) {
+  const float adx = fabsf(dx);
+  const float x = adx / r;
+  const float z = beta * sqrtf(fmaxf(1.0f - x * x, 0.0f));
+  const float dkb = -beta * beta * x * as_di0_over_z(z);  // d KB / d x
+  const float sgn = dx > 0.0f ? -1.0f : (dx < 0.0f ? 1.0f : 0.0f);  // sign(u - j)
+  return dkb * sgn / r;
+}
+
+// torch.remainder for float32 by a positive modulus (ungrid.py:873).
+__device__ __forceinline__ float remainder_f32(float a, float n) {
+  float m = fmodf(a, n);
+  if (m < 0.0f) m = __fadd_rn(m, n);
+  return m;
+}
+
+__device__ __forceinline__ int pos_mod(int a, int n) {
+  int m = a % n;
+  return m < 0 ? m + n : m;
+}
+
+// Balanced tile partition of [0, nos) into nt tiles: tile t = [b(t), b(t+1)),
+// b(t) = floor(t * nos / nt).
+__host__ __device__ __forceinline__ int tile_begin(int t, int nos, int nt) {
+  return (int)(((int64_t)t * nos) / nt);
+}
+__host__ __device__ __forceinline__ int tile_of(int s, int nos, int nt) {
+  return (int)((((int64_t)s + 1) * nt - 1) / nos);
+}
+
+}  // namespace mrn
+
+// Host-side plan object (defined in plan.cu).
+struct mrn_plan {
+  int ndim = 0;
+  int nslices = 0;
+  int flags = 0;
+  int device = 0;
+  double oversamp = 1.0;
+  double width[mrn::kMaxDim] = {1, 1, 1};
+  double beta = 0.0;
+  int tile[mrn::kMaxDim] = {1, 1, 1};
+  int coil_group = 1;
+  int max_coil = 1;
+  int max_chunk = 1024;
+  int tap_max = 8;  // compile-time tap bound used (8 or 16)
+  mrn::KBParams kb{};
+  std::vector<mrn::SliceGeom> h_slices;
+  int64_t n_img = 0, n_ksp = 0, n_grid = 0, n_trj = 0, n_pts = 0, n_x = 0;
+  int64_t n_prow = 0, n_irow = 0, n_xrow = 0;  // row counts of the grid / image layouts
+  int ntiles = 0;
+  int tmax_cells[mrn::kMaxDim] = {1, 1, 1};  // largest tile extent per dim over slices
+  int64_t n_entries_grid = 0;  // gridding entries of the bound trajectory
+  int64_t n_items_interp = 0, n_items_grid = 0, n_split = 0;
+  int64_t cap_entries = 0, cap_items_i = 0, cap_items_g = 0;  // allocated capacities
+  bool traj_set = false;
+
+  // device buffers
+  mrn::SliceGeom* d_slices = nullptr;
+  float* d_apod = nullptr;          // apodization tables
+  float4* d_coord_i = nullptr;      // interp-sorted scaled coords
+  int* d_perm_i = nullptr;          // interp-sorted global point ids
+  float4* d_coord_g = nullptr;      // gridding-sorted scaled coords
+  int* d_perm_g = nullptr;          // gridding-sorted global point ids
+  unsigned* d_key_a = nullptr;      // interp keys (unsorted)
+  unsigned* d_key_is = nullptr;     // interp keys (sorted)
+  unsigned* d_key_b = nullptr;      // gridding keys (unsorted)
+  unsigned* d_key_g = nullptr;      // gridding keys (sorted)
+  int* d_val_a = nullptr;
+  int* d_val_b = nullptr;
+  float4* d_coord_tmp = nullptr;    // unsorted coords
+  int* d_pt_slice = nullptr;        // point -> slice
+  int* d_entry_cnt = nullptr;       // per point gridding entries (scan input/output)
+  int* d_tile_start_i = nullptr;    // per global tile
+  int* d_tile_end_i = nullptr;
+  int* d_tile_start_g = nullptr;
+  int* d_tile_end_g = nullptr;
+  int* d_tile_nitems = nullptr;     // scan buffers
+  int* d_tile_item_off = nullptr;
+  mrn::Item* d_items_i = nullptr;
+  mrn::Item* d_items_g = nullptr;
+  int* d_counts = nullptr;          // [0] n_items_i [1] n_items_g [2] n_entries_g [3] n_split
+  int* d_split_tiles = nullptr;     // global tile ids of split gridding tiles
+  void* d_cub_tmp = nullptr;
+  size_t cub_tmp_bytes = 0;
+  float2* d_grid = nullptr;         // internal oversampled grid (natural order, grouped)
+  float2* d_ksp_tmp = nullptr;      // sample scratch for normal operators
+  unsigned* d_sync = nullptr;       // last-block counters
+  // FFT groups: slices with identical Nos share one batched cuFFT plan
+  struct FftGroup {
+    int nos[mrn::kMaxDim];
+    int64_t grid_off;   // complex offset in d_grid
+    int batch;          // sum of coils
+    cufftHandle handle;
+  };
+  std::vector<FftGroup> fft;
+
+  // Optional stage timing (mrn_plan_enable_timing): CUDA event pairs recorded
+  // on the launching stream around each stage, summed by mrn_plan_timing.
+  struct TimingRec {
+    int stage;
+    cudaEvent_t a, b;
+  };
+  bool timing = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<TimingRec> timing_recs;
+};
+
+namespace mrn {
+enum Stage { kStagePre = 0, kStageFft, kStageInterp, kStageGrid, kStagePost, kStageShift,
+             kStageTrajGrad, kStageCg, kNumStages };
+
+// Records a CUDA event pair around a scope when the plan's timing is on.
+struct StageTimer {
+  mrn_plan* P;
+  int idx = -1;
+  cudaStream_t st;
+  StageTimer(mrn_plan* p, int stage, cudaStream_t s);
+  ~StageTimer();
+};
+}  // namespace mrn

@@ -1,0 +1,34 @@
+// Internal launcher declarations (host side).
+#pragma once
+
+#include "common.cuh"
+
+namespace mrn {
+
+int cuda_fail(cudaError_t e);
+extern thread_local int g_last_cuda_error;
+
+// Which grid layout a tile kernel reads or writes.
+enum GridLayout { kInternal = 0, kUser = 1 };
+
+// Tile kernels (tiles.cu)
+int launch_interp(mrn_plan* P, const float2* grid, GridLayout layout, float2* ksp, float scale,
+                  const float2* temporal, cudaStream_t st);
+int launch_grid(mrn_plan* P, const float2* ksp, const float* dcf, GridLayout layout, float2* grid,
+                float scale, cudaStream_t st);
+int launch_grid_t(mrn_plan* P, const float2* ksp, const float* dcf, const float2* temporal,
+                  GridLayout layout, float2* grid, float scale, cudaStream_t st);
+int launch_traj_grad(mrn_plan* P, const float2* grid, GridLayout layout, const float2* samples,
+                     float* out, float scale, cudaStream_t st);
+
+// FFT-stage kernels (fftstage.cu)
+enum PreMode { kPrePlain = 0, kPreSense = 1 };
+int launch_pre(mrn_plan* P, PreMode mode, const float2* src, const float2* mps, float scale,
+               cudaStream_t st);
+enum PostMode { kPostPlain = 0, kPostSense = 1 };
+int launch_post(mrn_plan* P, PostMode mode, const float2* mps, float2* out, float scale,
+                const float2* xin, float lam, double* pap, int pap_stride, cudaStream_t st);
+int launch_shift_copy(mrn_plan* P, const float2* src, float2* dst, int to_user, cudaStream_t st);
+int run_fft(mrn_plan* P, int direction, cudaStream_t st);
+
+}  // namespace mrn

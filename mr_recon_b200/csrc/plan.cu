@@ -1,0 +1,702 @@
+// Plan creation and trajectory binning.
+//
+// A plan holds the geometry of n_slices NUFFT problems. mrn_plan_set_traj
+// turns a trajectory into the per-tile sample lists the tile kernels consume:
+//   interpolation: every sample belongs to the tile holding its first tap;
+//   gridding     : every sample is listed once for each tile its footprint
+//                  touches (1..2^d entries), so each tile owns its output.
+// Both lists are sorted by tile with a stable radix sort (samples keep their
+// trajectory order inside a tile) and cut into work items of at most
+// max_chunk samples. This replaces the per-call locs preparation of the
+// reference (prep_ungrid_shapes / prep_grid_shapes, ungrid.py:851-894,
+// grid.py:508-553) and has no counterpart in its Triton launch (one program
+// per point chunk, ungrid.py:127-129).
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+
+#include "common.cuh"
+#include "internal.cuh"
+
+using namespace mrn;
+
+namespace mrn {
+
+thread_local int g_last_cuda_error = 0;
+
+int cuda_fail(cudaError_t e) {
+  g_last_cuda_error = (int)e;
+  return e == cudaErrorMemoryAllocation ? MRN_ERR_NOMEM : MRN_ERR_CUDA;
+}
+
+__device__ __forceinline__ int find_slice_by_point(const SliceGeom* sl, int ns, int64_t p) {
+  int lo = 0, hi = ns - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (sl[mid].pt_off <= p) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ int find_slice_by_tile(const SliceGeom* sl, int ns, int t) {
+  int lo = 0, hi = ns - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (sl[mid].tile_base <= t) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Distinct tiles of one dimension touched by the valid taps of a sample at
+// wrapped coordinate u: taps j = lo + q, valid iff |(float)j - u| <= r (the
+// float32 mask of weights1d..3d, kernels.py:268-393), cell = j mod nos.
+__device__ __forceinline__ int dim_tiles(float u, float r, int ntaps, int nos, int nt,
+                                         int* tiles) {
+  const int lo = (int)ceilf(__fsub_rn(u, r));
+  int n = 0;
+  for (int q = 0; q < ntaps; ++q) {
+    const float dx = __fsub_rn((float)(lo + q), u);
+    if (!(fabsf(dx) <= r)) continue;
+    const int t = nt == 1 ? 0 : tile_of(pos_mod(lo + q, nos), nos, nt);
+    bool seen = false;
+    for (int z = 0; z < n; ++z) seen |= (tiles[z] == t);
+    if (!seen) tiles[n++] = t;
+  }
+  return n;
+}
+
+// Per sample: scaled, wrapped coordinates (fourier.py:420-430 then
+// ungrid.py:873), interpolation tile key (tile of the first candidate tap),
+// and the number of gridding tiles its footprint touches.
+__global__ void k_prep_points(const SliceGeom* __restrict__ sl, int ns, int ndim, KBParams kb,
+                              const float* __restrict__ trj, int64_t npts,
+                              float4* __restrict__ coord, unsigned* __restrict__ key_i,
+                              int* __restrict__ val_i, int* __restrict__ ecnt) {
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npts) return;
+  const int s = find_slice_by_point(sl, ns, p);
+  const SliceGeom& g = sl[s];
+  const int64_t lp = p - g.pt_off;
+  float u[kMaxDim] = {0.f, 0.f, 0.f};
+  int lin = 0;
+  int ntouch = 1;
+  for (int i = 0; i < ndim; ++i) {
+    const float k = trj[(g.pt_off + lp) * ndim + i];
+    float v = __fadd_rn(__fmul_rn(k, g.scale[i]), g.shift[i]);
+    v = remainder_f32(v, (float)g.nos[i]);
+    u[i] = v;
+    const int lo = (int)ceilf(__fsub_rn(v, kb.radius[i]));
+    const int t0 = tile_of(pos_mod(lo, g.nos[i]), g.nos[i], g.ntile[i]);
+    lin = lin * g.ntile[i] + t0;
+    int tiles[kMaxTaps];
+    ntouch *= dim_tiles(v, kb.radius[i], kb.ntaps[i], g.nos[i], g.ntile[i], tiles);
+  }
+  coord[p] = make_float4(u[0], u[1], u[2], 0.f);
+  key_i[p] = (unsigned)(g.tile_base + lin);
+  val_i[p] = (int)p;
+  ecnt[p] = ntouch;
+}
+
+// Emit (tile, point) gridding entries at the scanned offsets.
+__global__ void k_emit_entries(const SliceGeom* __restrict__ sl, int ns, int ndim, KBParams kb,
+                               const float4* __restrict__ coord, int64_t npts,
+                               const int* __restrict__ eoff, unsigned* __restrict__ key,
+                               int* __restrict__ val) {
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npts) return;
+  const int s = find_slice_by_point(sl, ns, p);
+  const SliceGeom& g = sl[s];
+  const float4 c4 = coord[p];
+  const float uu[3] = {c4.x, c4.y, c4.z};
+  int tiles[kMaxDim][kMaxTaps];
+  int nt[kMaxDim] = {1, 1, 1};
+  for (int i = 0; i < ndim; ++i)
+    nt[i] = dim_tiles(uu[i], kb.radius[i], kb.ntaps[i], g.nos[i], g.ntile[i], tiles[i]);
+  int o = eoff[p];
+  for (int a = 0; a < nt[0]; ++a)
+    for (int b = 0; b < (ndim > 1 ? nt[1] : 1); ++b)
+      for (int c = 0; c < (ndim > 2 ? nt[2] : 1); ++c) {
+        int lin = tiles[0][a];
+        if (ndim > 1) lin = lin * g.ntile[1] + tiles[1][b];
+        if (ndim > 2) lin = lin * g.ntile[2] + tiles[2][c];
+        key[o] = (unsigned)(g.tile_base + lin);
+        val[o] = (int)p;
+        ++o;
+      }
+}
+
+__global__ void k_gather_coords(const float4* __restrict__ src, const int* __restrict__ perm,
+                                int64_t n, float4* __restrict__ dst) {
+  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) dst[e] = src[perm[e]];
+}
+
+__global__ void k_tile_ranges(const unsigned* __restrict__ key, int64_t n, int ntiles,
+                              int* __restrict__ start, int* __restrict__ end) {
+  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const unsigned k = key[e];
+  if ((int)k >= ntiles) return;
+  if (e == 0 || key[e - 1] != k) start[k] = (int)e;
+  if (e == n - 1 || key[e + 1] != k) end[k] = (int)(e + 1);
+}
+
+__global__ void k_item_counts(const int* __restrict__ start, const int* __restrict__ end,
+                              int ntiles, int chunk, int min_items, int* __restrict__ nitems) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntiles) return;
+  const int c = end[t] - start[t];
+  nitems[t] = max(min_items, (c + chunk - 1) / chunk);
+}
+
+__global__ void k_emit_items(const SliceGeom* __restrict__ sl, int ns, const int* __restrict__ start,
+                             const int* __restrict__ end, const int* __restrict__ nitems,
+                             const int* __restrict__ ioff, int ntiles, int chunk,
+                             Item* __restrict__ items, int* __restrict__ split_tiles,
+                             int* __restrict__ counts, int count_slot, int split_slot) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntiles) return;
+  const int n = nitems[t];
+  const int s = find_slice_by_tile(sl, ns, t);
+  const int c = end[t] - start[t];
+  for (int q = 0; q < n; ++q) {
+    Item it;
+    it.slice = s;
+    it.tile = t - sl[s].tile_base;
+    it.start = start[t] + q * chunk;
+    it.count = max(0, min(chunk, c - q * chunk));
+    it.split = n > 1 ? 1 : 0;
+    it.pad[0] = it.pad[1] = it.pad[2] = 0;
+    items[ioff[t] + q] = it;
+  }
+  if (t == ntiles - 1) counts[count_slot] = ioff[t] + n;
+  if (split_slot >= 0 && n > 1) {
+    const int k = atomicAdd(&counts[split_slot], 1);
+    split_tiles[k] = t;
+  }
+}
+
+__global__ void k_total(const int* __restrict__ off, const int* __restrict__ cnt, int64_t n,
+                        int* __restrict__ out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *out = n > 0 ? off[n - 1] + cnt[n - 1] : 0;
+}
+
+static inline unsigned blocks_for(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+static cudaEvent_t pool_event(mrn_plan* P) {
+  if (!P->ev_pool.empty()) {
+    cudaEvent_t e = P->ev_pool.back();
+    P->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+  return e;
+}
+
+StageTimer::StageTimer(mrn_plan* p, int stage, cudaStream_t s) : P(p), st(s) {
+  if (!P || !P->timing) return;
+  mrn_plan::TimingRec r{stage, pool_event(P), pool_event(P)};
+  if (!r.a || !r.b) return;
+  cudaEventRecord(r.a, st);
+  P->timing_recs.push_back(r);
+  idx = (int)P->timing_recs.size() - 1;
+}
+
+StageTimer::~StageTimer() {
+  if (idx >= 0) cudaEventRecord(P->timing_recs[idx].b, st);
+}
+
+template <class T>
+static int dev_alloc(T** p, size_t n) {
+  if (*p) { cudaFree(*p); *p = nullptr; }
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e != cudaSuccess) return cuda_fail(e);
+  return MRN_OK;
+}
+
+static int ensure_cub(mrn_plan* P, size_t bytes) {
+  if (bytes <= P->cub_tmp_bytes && P->d_cub_tmp) return MRN_OK;
+  if (P->d_cub_tmp) cudaFree(P->d_cub_tmp);
+  P->d_cub_tmp = nullptr;
+  cudaError_t e = cudaMalloc(&P->d_cub_tmp, bytes);
+  if (e != cudaSuccess) return cuda_fail(e);
+  P->cub_tmp_bytes = bytes;
+  return MRN_OK;
+}
+
+}  // namespace mrn
+
+#define CK(x)                                   \
+  do {                                          \
+    cudaError_t _e = (x);                       \
+    if (_e != cudaSuccess) return cuda_fail(_e); \
+  } while (0)
+#define RK(x)                  \
+  do {                         \
+    int _r = (x);              \
+    if (_r != MRN_OK) return _r; \
+  } while (0)
+
+extern "C" {
+
+const char* mrn_version(void) { return "mrnufft 0.1.0 (sm_100a)"; }
+
+const char* mrn_error_string(int code) {
+  switch (code) {
+    case MRN_OK: return "ok";
+    case MRN_ERR_ARG: return "invalid argument";
+    case MRN_ERR_WIDTH: return "kernel width out of range (1 <= width < 16)";
+    case MRN_ERR_CUDA: return "CUDA error";
+    case MRN_ERR_CUFFT: return "cuFFT error";
+    case MRN_ERR_NOMEM: return "device allocation failed";
+    case MRN_ERR_STATE: return "trajectory not set on plan";
+    case MRN_ERR_UNSUPPORTED: return "unsupported configuration";
+    default: return "unknown error";
+  }
+}
+
+int mrn_last_cuda_error(void) { return mrn::g_last_cuda_error; }
+
+int mrn_plan_create(mrn_plan** out, int ndim, int n_slices, const int* im_size,
+                    const int64_t* n_pts, const int* n_coil, double oversamp,
+                    const double* width, double beta, int flags, const int* tile,
+                    int coil_group, int max_chunk, int device) {
+  if (!out || !im_size || !n_pts || !n_coil || !width) return MRN_ERR_ARG;
+  *out = nullptr;
+  if (ndim < 1 || ndim > kMaxDim || n_slices < 1) return MRN_ERR_ARG;
+  const bool raw = (flags & MRN_PLAN_RAW) != 0;
+  if (!raw && !(oversamp >= 1.0)) return MRN_ERR_ARG;
+  for (int i = 0; i < ndim; ++i)
+    if (!(width[i] >= 1.0) || !(width[i] < (double)kMaxTaps)) return MRN_ERR_WIDTH;
+  if (tile)
+    for (int i = 0; i < ndim; ++i)
+      if (tile[i] < 1) return MRN_ERR_ARG;
+  if (coil_group < 0 || max_chunk < 0) return MRN_ERR_ARG;
+
+  mrn_plan* P = new mrn_plan();
+  P->ndim = ndim;
+  P->nslices = n_slices;
+  P->flags = flags;
+  P->device = device;
+  P->oversamp = raw ? 1.0 : oversamp;
+  int maxtaps = 0;
+  for (int i = 0; i < ndim; ++i) {
+    P->width[i] = width[i];
+    P->kb.radius[i] = (float)width[i] / 2.0f;
+    P->kb.ntaps[i] = (int)std::floor(width[i]) + 1;
+    maxtaps = std::max(maxtaps, P->kb.ntaps[i]);
+  }
+  P->tap_max = maxtaps <= 8 ? 8 : 16;
+  if (beta <= 0.0) {
+    if (raw) { delete P; return MRN_ERR_ARG; }
+    const double w = width[0];
+    beta = M_PI * std::sqrt(std::pow(w / oversamp * (oversamp - 0.5), 2) - 0.8);
+  }
+  P->beta = beta;
+  P->kb.beta = (float)beta;
+
+  int maxc = 0;
+  for (int s = 0; s < n_slices; ++s) {
+    if (n_coil[s] < 1 || n_pts[s] < 0) { delete P; return MRN_ERR_ARG; }
+    for (int i = 0; i < ndim; ++i)
+      if (im_size[s * ndim + i] < 1) { delete P; return MRN_ERR_ARG; }
+    maxc = std::max(maxc, n_coil[s]);
+  }
+  P->max_coil = maxc;
+
+  // Built-in tile choice: 2D 16x16... chosen so tile + halo stays modest.
+  int deftile[kMaxDim];
+  for (int i = 0; i < ndim; ++i) deftile[i] = (ndim == 1) ? 256 : (ndim == 2 ? 16 : 8);
+  for (int i = 0; i < ndim; ++i) P->tile[i] = tile ? tile[i] : deftile[i];
+  P->max_chunk = max_chunk > 0 ? max_chunk : 1024;
+
+  // Slices
+  int64_t img = 0, ksp = 0, ugrid = 0, trjo = 0, pts = 0, xo = 0;
+  int64_t prow = 0, irow = 0, xrow = 0;
+  int tiles = 0;
+  int64_t maxe = 0;
+  int64_t apodn = 0;
+  P->h_slices.resize(n_slices);
+  for (int s = 0; s < n_slices; ++s) {
+    SliceGeom& g = P->h_slices[s];
+    std::memset(&g, 0, sizeof(g));
+    int64_t nimg = 1, gos = 1, spans = 1;
+    for (int i = 0; i < kMaxDim; ++i) {
+      g.n[i] = 1; g.nos[i] = 1; g.ntile[i] = 1; g.hshift[i] = 0; g.scale[i] = 1.f; g.shift[i] = 0.f;
+    }
+    int tcount = 1;
+    for (int i = 0; i < ndim; ++i) {
+      const int n = im_size[s * ndim + i];
+      const int nos = raw ? n : (int)std::ceil(oversamp * n);
+      g.n[i] = n;
+      g.nos[i] = nos;
+      g.hshift[i] = raw ? 0 : nos / 2;
+      g.scale[i] = raw ? 1.0f : (float)((double)nos / (double)n);
+      g.shift[i] = raw ? 0.0f : (float)(nos / 2);
+      const int K = P->kb.ntaps[i];
+      // tiles: at most ceil(nos / tile); each tile at least K-1 cells wide so a
+      // footprint touches at most two tiles per dimension
+      int nt = (nos + P->tile[i] - 1) / P->tile[i];
+      if (K > 1) nt = std::min(nt, std::max(1, nos / (K - 1)));
+      nt = std::max(1, nt);
+      g.ntile[i] = nt;
+      tcount *= nt;
+      nimg *= n;
+      gos *= nos;
+      spans *= (nt == 1 ? 1 : 2);
+      P->tmax_cells[i] = std::max(P->tmax_cells[i], (nos + nt - 1) / nt);
+      g.apod_off[i] = (int)apodn;
+      apodn += n;
+    }
+    g.tile_base = tiles;
+    g.ncoil = n_coil[s];
+    g.m = n_pts[s];
+    g.pt_off = pts;
+    g.img_off = img;
+    g.ksp_off = ksp;
+    g.ugrid_off = ugrid;
+    g.x_off = xo;
+    g.gos = gos;
+    g.nimg = nimg;
+    g.inv_sqrt_n = (float)(1.0 / std::sqrt((double)nimg));
+    g.prow_off = prow;
+    g.irow_off = irow;
+    g.xrow_off = xrow;
+    prow += (int64_t)g.ncoil * gos / g.nos[ndim - 1];
+    irow += (int64_t)g.ncoil * nimg / g.n[ndim - 1];
+    xrow += nimg / g.n[ndim - 1];
+    tiles += tcount;
+    img += (int64_t)g.ncoil * nimg;
+    ksp += (int64_t)g.ncoil * g.m;
+    ugrid += (int64_t)g.ncoil * gos;
+    trjo += g.m * ndim;
+    pts += g.m;
+    xo += nimg;
+    maxe += spans * g.m;
+  }
+  P->n_img = img;
+  P->n_ksp = ksp;
+  P->n_grid = ugrid;
+  P->n_trj = trjo;
+  P->n_pts = pts;
+  P->n_x = xo;
+  P->n_prow = prow;
+  P->n_irow = irow;
+  P->n_xrow = xrow;
+  P->ntiles = tiles;
+  if (pts >= (int64_t)INT32_MAX || maxe >= (int64_t)INT32_MAX) { delete P; return MRN_ERR_UNSUPPORTED; }
+
+  // Coil group: all coils of the widest slice, limited by shared memory.
+  if (coil_group > 0) {
+    P->coil_group = std::min(coil_group, 64);
+  } else {
+    int64_t cells = 1;
+    for (int i = 0; i < ndim; ++i) cells *= (P->tmax_cells[i] + P->kb.ntaps[i] - 1);
+    const int64_t budget = 96 * 1024;  // bytes of tile data per CTA, two CTAs per SM
+    int cg = (int)std::max<int64_t>(1, budget / ((cells | 1) * 8));
+    cg = std::min(cg, 64);
+    cg = std::min(cg, maxc);
+    // balance groups: same number of groups, fewest coils per group
+    const int ngroups = (maxc + cg - 1) / cg;
+    cg = (maxc + ngroups - 1) / ngroups;
+    P->coil_group = std::max(1, cg);
+  }
+
+  // FFT groups in first-seen order; internal grid buffer ordered by group.
+  if (!raw) {
+    std::vector<int> group_of(n_slices, -1);
+    for (int s = 0; s < n_slices; ++s) {
+      const SliceGeom& g = P->h_slices[s];
+      int found = -1;
+      for (size_t q = 0; q < P->fft.size(); ++q) {
+        bool same = true;
+        for (int i = 0; i < ndim; ++i) same &= (P->fft[q].nos[i] == g.nos[i]);
+        if (same) { found = (int)q; break; }
+      }
+      if (found < 0) {
+        mrn_plan::FftGroup fg{};
+        for (int i = 0; i < kMaxDim; ++i) fg.nos[i] = g.nos[i];
+        fg.batch = 0;
+        fg.handle = 0;
+        P->fft.push_back(fg);
+        found = (int)P->fft.size() - 1;
+      }
+      group_of[s] = found;
+      P->fft[found].batch += g.ncoil;
+    }
+    int64_t off = 0;
+    for (size_t q = 0; q < P->fft.size(); ++q) {
+      P->fft[q].grid_off = off;
+      for (int s = 0; s < n_slices; ++s)
+        if (group_of[s] == (int)q) {
+          P->h_slices[s].grid_off = off;
+          off += (int64_t)P->h_slices[s].ncoil * P->h_slices[s].gos;
+        }
+    }
+  } else {
+    for (int s = 0; s < n_slices; ++s) P->h_slices[s].grid_off = P->h_slices[s].ugrid_off;
+  }
+
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) { delete P; return cuda_fail(e); }
+
+  int rc = MRN_OK;
+#define PK(x) do { rc = (x); if (rc != MRN_OK) { mrn_plan_destroy(P); return rc; } } while (0)
+  PK(dev_alloc(&P->d_slices, n_slices));
+  e = cudaMemcpy(P->d_slices, P->h_slices.data(), n_slices * sizeof(SliceGeom), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { mrn_plan_destroy(P); return cuda_fail(e); }
+
+  // Apodization tables a(x) = sqrt(beta^2 - (pi W x)^2) / sinh(.), x = (q - N//2)/Nos
+  // (fourier.py:376-418), in double then rounded.
+  {
+    std::vector<float> ap(std::max<int64_t>(apodn, 1), 1.0f);
+    if (!raw && !(flags & MRN_PLAN_NO_APOD)) {
+      for (int s = 0; s < n_slices; ++s) {
+        const SliceGeom& g = P->h_slices[s];
+        for (int i = 0; i < ndim; ++i) {
+          for (int q = 0; q < g.n[i]; ++q) {
+            const double x = (double)(q - g.n[i] / 2) / (double)g.nos[i];
+            const double t = M_PI * P->width[i] * x;
+            const double a = std::sqrt(beta * beta - t * t);
+            ap[g.apod_off[i] + q] = (float)(a / std::sinh(a));
+          }
+        }
+      }
+    }
+    PK(dev_alloc(&P->d_apod, ap.size()));
+    e = cudaMemcpy(P->d_apod, ap.data(), ap.size() * sizeof(float), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { mrn_plan_destroy(P); return cuda_fail(e); }
+  }
+
+  const int64_t np = std::max<int64_t>(pts, 1);
+  PK(dev_alloc(&P->d_coord_i, np));
+  PK(dev_alloc(&P->d_perm_i, np));
+  PK(dev_alloc(&P->d_coord_tmp, np));
+  PK(dev_alloc(&P->d_entry_cnt, 2 * np));
+  PK(dev_alloc(&P->d_key_a, np));
+  PK(dev_alloc(&P->d_val_a, np));
+  PK(dev_alloc(&P->d_key_is, np));
+  PK(dev_alloc(&P->d_tile_start_i, tiles));
+  PK(dev_alloc(&P->d_tile_end_i, tiles));
+  PK(dev_alloc(&P->d_tile_start_g, tiles));
+  PK(dev_alloc(&P->d_tile_end_g, tiles));
+  PK(dev_alloc(&P->d_tile_nitems, tiles));
+  PK(dev_alloc(&P->d_tile_item_off, tiles));
+  PK(dev_alloc(&P->d_counts, 8));
+  PK(dev_alloc(&P->d_split_tiles, tiles));
+  PK(dev_alloc(&P->d_sync, 64));
+  CK(cudaMemset(P->d_sync, 0, 64 * sizeof(unsigned)));
+  if (!raw) {
+    PK(dev_alloc(&P->d_grid, std::max<int64_t>(P->n_grid, 1)));
+    PK(dev_alloc(&P->d_ksp_tmp, std::max<int64_t>(P->n_ksp, 1)));
+    for (auto& fg : P->fft) {
+      int n[kMaxDim];
+      for (int i = 0; i < ndim; ++i) n[i] = fg.nos[i];
+      cufftResult r = cufftPlanMany(&fg.handle, ndim, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C,
+                                    fg.batch);
+      if (r != CUFFT_SUCCESS) { fg.handle = 0; mrn_plan_destroy(P); return MRN_ERR_CUFFT; }
+    }
+  }
+#undef PK
+  *out = P;
+  return MRN_OK;
+}
+
+int mrn_plan_enable_timing(mrn_plan* P, int on) {
+  if (!P) return MRN_ERR_ARG;
+  P->timing = on != 0;
+  return MRN_OK;
+}
+
+int mrn_plan_timing(mrn_plan* P, double* ms, int64_t* count) {
+  if (!P || !ms || !count) return MRN_ERR_ARG;
+  for (int i = 0; i < kNumStages; ++i) { ms[i] = 0.0; count[i] = 0; }
+  int rc = MRN_OK;
+  for (auto& r : P->timing_recs) {
+    cudaError_t e = cudaEventSynchronize(r.b);
+    float t = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, r.a, r.b);
+    if (e != cudaSuccess) rc = cuda_fail(e);
+    else if (r.stage >= 0 && r.stage < kNumStages) { ms[r.stage] += t; count[r.stage] += 1; }
+    P->ev_pool.push_back(r.a);
+    P->ev_pool.push_back(r.b);
+  }
+  P->timing_recs.clear();
+  return rc;
+}
+
+int mrn_plan_destroy(mrn_plan* P) {
+  if (!P) return MRN_OK;
+  for (auto& r : P->timing_recs) { P->ev_pool.push_back(r.a); P->ev_pool.push_back(r.b); }
+  for (cudaEvent_t e : P->ev_pool)
+    if (e) cudaEventDestroy(e);
+  for (auto& fg : P->fft)
+    if (fg.handle) cufftDestroy(fg.handle);
+  void* bufs[] = {P->d_slices, P->d_apod, P->d_coord_i, P->d_perm_i, P->d_coord_g, P->d_perm_g,
+                  P->d_key_a, P->d_key_b, P->d_key_is, P->d_key_g, P->d_val_a, P->d_val_b, P->d_coord_tmp,
+                  P->d_entry_cnt, P->d_tile_start_i, P->d_tile_end_i, P->d_tile_start_g,
+                  P->d_tile_end_g, P->d_tile_nitems, P->d_tile_item_off, P->d_items_i,
+                  P->d_items_g, P->d_counts, P->d_split_tiles, P->d_cub_tmp, P->d_grid,
+                  P->d_ksp_tmp, P->d_sync};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+  delete P;
+  return MRN_OK;
+}
+
+int mrn_plan_offsets(const mrn_plan* P, int64_t* img_off, int64_t* ksp_off, int64_t* grid_off,
+                     int64_t* trj_off) {
+  if (!P) return MRN_ERR_ARG;
+  for (int s = 0; s < P->nslices; ++s) {
+    const SliceGeom& g = P->h_slices[s];
+    if (img_off) img_off[s] = g.img_off;
+    if (ksp_off) ksp_off[s] = g.ksp_off;
+    if (grid_off) grid_off[s] = g.ugrid_off;
+    if (trj_off) trj_off[s] = g.pt_off * P->ndim;
+  }
+  return MRN_OK;
+}
+
+int mrn_plan_sizes(const mrn_plan* P, int64_t* o) {
+  if (!P || !o) return MRN_ERR_ARG;
+  o[0] = P->n_img; o[1] = P->n_ksp; o[2] = P->n_grid; o[3] = P->n_trj; o[4] = P->ntiles;
+  o[5] = P->h_slices[0].nos[0]; o[6] = P->h_slices[0].nos[1]; o[7] = P->h_slices[0].nos[2];
+  return MRN_OK;
+}
+
+int mrn_plan_stats(mrn_plan* P, int64_t* o) {
+  if (!P || !o) return MRN_ERR_ARG;
+  o[0] = P->n_items_interp; o[1] = P->n_items_grid; o[2] = P->n_entries_grid; o[3] = P->n_split;
+  return MRN_OK;
+}
+
+int mrn_plan_set_traj(mrn_plan* P, const float* trj, void* stream_) {
+  if (!P || (!trj && P->n_pts > 0)) return MRN_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream_;
+  const int64_t M = P->n_pts;
+  const int T = P->ntiles;
+  const int ndim = P->ndim;
+  int bits = 1;
+  while (bits < 31 && (1ll << bits) <= (long long)T) ++bits;
+  P->traj_set = false;
+
+  // 1. coordinates, interpolation keys, gridding entry counts
+  int* eoff = P->d_entry_cnt + std::max<int64_t>(M, 1);
+  size_t need = 0, b = 0;
+  const int Mi = (int)std::max<int64_t>(M, 1);
+  cub::DeviceScan::ExclusiveSum(nullptr, b, P->d_entry_cnt, eoff, Mi, st);
+  need = std::max(need, b);
+  cub::DeviceScan::ExclusiveSum(nullptr, b, P->d_tile_nitems, P->d_tile_item_off, T, st);
+  need = std::max(need, b);
+  cub::DeviceRadixSort::SortPairs(nullptr, b, P->d_key_a, P->d_key_is, P->d_val_a, P->d_perm_i,
+                                  Mi, 0, bits, st);
+  need = std::max(need, b);
+  RK(ensure_cub(P, need));
+
+  int64_t E = 0;
+  if (M > 0) {
+    k_prep_points<<<blocks_for(M), 256, 0, st>>>(P->d_slices, P->nslices, ndim, P->kb, trj, M,
+                                                  P->d_coord_tmp, P->d_key_a, P->d_val_a,
+                                                  P->d_entry_cnt);
+    CK(cudaGetLastError());
+    b = P->cub_tmp_bytes;
+    CK(cub::DeviceScan::ExclusiveSum(P->d_cub_tmp, b, P->d_entry_cnt, eoff, (int)M, st));
+    k_total<<<1, 32, 0, st>>>(eoff, P->d_entry_cnt, M, P->d_counts + 2);
+    CK(cudaGetLastError());
+    int hE = 0;
+    CK(cudaMemcpyAsync(&hE, P->d_counts + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    E = hE;
+  }
+  P->n_entries_grid = E;
+
+  // 2. gridding entry buffers grow on demand
+  const int64_t capE = std::max<int64_t>(E, 1);
+  if (P->cap_entries < capE) {
+    RK(dev_alloc(&P->d_key_b, (size_t)capE));
+    RK(dev_alloc(&P->d_val_b, (size_t)capE));
+    RK(dev_alloc(&P->d_key_g, (size_t)capE));
+    RK(dev_alloc(&P->d_perm_g, (size_t)capE));
+    RK(dev_alloc(&P->d_coord_g, (size_t)capE));
+    P->cap_entries = capE;
+  }
+
+  // 3. emit gridding entries and sort both lists by tile (stable)
+  if (M > 0) {
+    k_emit_entries<<<blocks_for(M), 256, 0, st>>>(P->d_slices, P->nslices, ndim, P->kb,
+                                                   P->d_coord_tmp, M, eoff, P->d_key_b, P->d_val_b);
+    CK(cudaGetLastError());
+    b = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, b, P->d_key_b, P->d_key_g, P->d_val_b, P->d_perm_g,
+                                    (int)std::max<int64_t>(E, 1), 0, bits, st);
+    RK(ensure_cub(P, std::max(b, P->cub_tmp_bytes)));
+    b = P->cub_tmp_bytes;
+    CK(cub::DeviceRadixSort::SortPairs(P->d_cub_tmp, b, P->d_key_a, P->d_key_is, P->d_val_a,
+                                       P->d_perm_i, (int)M, 0, bits, st));
+    b = P->cub_tmp_bytes;
+    CK(cub::DeviceRadixSort::SortPairs(P->d_cub_tmp, b, P->d_key_b, P->d_key_g, P->d_val_b,
+                                       P->d_perm_g, (int)E, 0, bits, st));
+    k_gather_coords<<<blocks_for(M), 256, 0, st>>>(P->d_coord_tmp, P->d_perm_i, M, P->d_coord_i);
+    if (E > 0)
+      k_gather_coords<<<blocks_for(E), 256, 0, st>>>(P->d_coord_tmp, P->d_perm_g, E, P->d_coord_g);
+    CK(cudaGetLastError());
+  }
+
+  // 4. per-tile ranges and work items
+  CK(cudaMemsetAsync(P->d_tile_start_i, 0, T * sizeof(int), st));
+  CK(cudaMemsetAsync(P->d_tile_end_i, 0, T * sizeof(int), st));
+  CK(cudaMemsetAsync(P->d_tile_start_g, 0, T * sizeof(int), st));
+  CK(cudaMemsetAsync(P->d_tile_end_g, 0, T * sizeof(int), st));
+  CK(cudaMemsetAsync(P->d_counts, 0, 8 * sizeof(int), st));
+  if (M > 0) {
+    k_tile_ranges<<<blocks_for(M), 256, 0, st>>>(P->d_key_is, M, T, P->d_tile_start_i,
+                                                 P->d_tile_end_i);
+    if (E > 0)
+      k_tile_ranges<<<blocks_for(E), 256, 0, st>>>(P->d_key_g, E, T, P->d_tile_start_g,
+                                                   P->d_tile_end_g);
+  }
+  const int chunk = P->max_chunk;
+  const int64_t max_items_i = (int64_t)T + M / chunk + 1;
+  const int64_t max_items_g = (int64_t)T + E / chunk + 1;
+  if (P->cap_items_i < max_items_i) {
+    RK(dev_alloc(&P->d_items_i, (size_t)max_items_i));
+    P->cap_items_i = max_items_i;
+  }
+  if (P->cap_items_g < max_items_g) {
+    RK(dev_alloc(&P->d_items_g, (size_t)max_items_g));
+    P->cap_items_g = max_items_g;
+  }
+  k_item_counts<<<blocks_for(T), 256, 0, st>>>(P->d_tile_start_i, P->d_tile_end_i, T, chunk, 0,
+                                               P->d_tile_nitems);
+  b = P->cub_tmp_bytes;
+  CK(cub::DeviceScan::ExclusiveSum(P->d_cub_tmp, b, P->d_tile_nitems, P->d_tile_item_off, T, st));
+  k_emit_items<<<blocks_for(T), 256, 0, st>>>(P->d_slices, P->nslices, P->d_tile_start_i,
+                                              P->d_tile_end_i, P->d_tile_nitems, P->d_tile_item_off,
+                                              T, chunk, P->d_items_i, nullptr, P->d_counts, 0, -1);
+  k_item_counts<<<blocks_for(T), 256, 0, st>>>(P->d_tile_start_g, P->d_tile_end_g, T, chunk, 1,
+                                               P->d_tile_nitems);
+  b = P->cub_tmp_bytes;
+  CK(cub::DeviceScan::ExclusiveSum(P->d_cub_tmp, b, P->d_tile_nitems, P->d_tile_item_off, T, st));
+  k_emit_items<<<blocks_for(T), 256, 0, st>>>(P->d_slices, P->nslices, P->d_tile_start_g,
+                                              P->d_tile_end_g, P->d_tile_nitems, P->d_tile_item_off,
+                                              T, chunk, P->d_items_g, P->d_split_tiles, P->d_counts,
+                                              1, 3);
+  CK(cudaGetLastError());
+  int hc[4] = {0, 0, 0, 0};
+  CK(cudaMemcpyAsync(hc, P->d_counts, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  P->n_items_interp = hc[0];
+  P->n_items_grid = hc[1];
+  P->n_split = hc[3];
+  P->traj_set = true;
+  return MRN_OK;
+}
+
+}  // extern "C"

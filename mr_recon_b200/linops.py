@@ -1,0 +1,186 @@
+"""Linear operators with the interface of mr_recon's linops.py (``linop``,
+``batching_params``, ``sense_linop``, linops.py:22-47 and 1041-1308).
+
+``sense_linop`` keeps the reference constructor and shapes. With the B200
+NUFFT (the default here) and no time segmentation, forward / adjoint /
+normal each run as one fused pass over all coils: coil maps are multiplied
+inside the pre-FFT kernel, the density compensation inside the gridding
+kernel, and conj(coil map) summation inside the post-iFFT kernel, where the
+reference loops over coil and segment batches in Python
+(linops.py:1160-1176, 1206-1226).
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import Optional
+
+import torch
+import torch.nn as nn
+from einops import einsum, rearrange
+
+from . import _lib
+from .fourier import NUFFT, b200_nufft
+from .plan import Plan
+from .utils import PadLast, batch_iterator, fft, ifft
+
+complex_dtype = torch.complex64
+real_dtype = torch.float32
+
+__all__ = ["batching_params", "linop", "sense_linop"]
+
+
+@dataclass
+class batching_params:
+    """Batch sizes (linops.py:22-28). The fused B200 path ignores them: all
+    coils and segments run in one launch."""
+    coil_batch_size: Optional[int] = 1
+    sub_batch_size: Optional[int] = 1
+    field_batch_size: Optional[int] = 1
+    toeplitz_batch_size: Optional[int] = 1
+    img_batch_size: Optional[int] = 1
+
+
+class linop(nn.Module):
+    """Generic linop (linops.py:30-47)."""
+
+    def __init__(self, ishape, oshape):
+        super().__init__()
+        self.ishape = ishape
+        self.oshape = oshape
+
+    def forward(self, *args):
+        raise NotImplementedError
+
+    def adjoint(self, *args):
+        raise NotImplementedError
+
+    def normal(self, *args):
+        raise NotImplementedError
+
+
+class sense_linop(linop):
+    """SENSE model y_c = sum_l h_l * F(S_c * b_l * x) (linops.py:1041-1308)."""
+
+    def __init__(self, trj: torch.Tensor, mps: torch.Tensor, dcf: Optional[torch.Tensor] = None,
+                 nufft: Optional[NUFFT] = None, use_toeplitz: Optional[bool] = False,
+                 spatial_funcs: Optional[torch.Tensor] = None,
+                 temporal_funcs: Optional[torch.Tensor] = None,
+                 bparams: Optional[batching_params] = batching_params()):
+        im_size = tuple(mps.shape[1:])
+        trj_size = tuple(trj.shape[:-1])
+        ncoils = mps.shape[0]
+        super().__init__(im_size, (ncoils, *trj_size))
+        dev = trj.device
+        assert mps.device == dev
+        _lib.require_cuda(trj, "trajectory")
+        if nufft is None:
+            nufft = b200_nufft(im_size)
+        self.segmented = spatial_funcs is not None or temporal_funcs is not None
+        if dcf is None:
+            dcf = torch.ones(trj_size, dtype=real_dtype, device=dev)
+        if spatial_funcs is None:
+            spatial_funcs = torch.ones((1,) * (len(im_size) + 1), dtype=complex_dtype, device=dev)
+        if temporal_funcs is None:
+            temporal_funcs = torch.ones((1,) * (len(trj_size) + 1), dtype=complex_dtype, device=dev)
+        trj = nufft.rescale_trajectory(trj).type(real_dtype)
+        dcf = dcf.type(real_dtype).contiguous()
+        mps = mps.type(complex_dtype).contiguous()
+
+        self.im_size = im_size
+        self.trj_size = trj_size
+        self.use_toeplitz = use_toeplitz
+        self.trj = trj
+        self.mps = mps
+        self.dcf = dcf
+        self.nufft = nufft
+        self.bparams = bparams
+        self.spatial_funcs = spatial_funcs
+        self.temporal_funcs = temporal_funcs
+        self.torch_dev = dev
+
+        # fused single-pass plan (B200 NUFFT, no time segmentation)
+        self.plan = None
+        if isinstance(nufft, b200_nufft) and not self.segmented:
+            M = 1
+            for s in trj_size:
+                M *= int(s)
+            self.plan = Plan([im_size], [M], [ncoils], nufft.oversamp, nufft._widths(), nufft.beta,
+                             apodize=nufft.apodize, tile=nufft.tile, coil_group=nufft.coil_group,
+                             max_chunk=nufft.max_chunk, device=dev)
+            self.plan.set_traj(trj.contiguous())
+
+        if use_toeplitz:
+            # linops.py:1102-1119: the spatial/temporal defaults are already in
+            # place here, so the reference always builds (L, L, *im_os) kernels
+            tf = temporal_funcs.to(complex_dtype)
+            weights = einsum(tf.conj(), tf, "L1 ... , L2 ... -> L1 L2 ...")
+            weights = rearrange(weights, "n1 n2 ... -> (n1 n2) ... ") * dcf[None, ...]
+            kerns = []
+            for b1 in range(0, weights.shape[0], bparams.toeplitz_batch_size):
+                b2 = min(b1 + bparams.toeplitz_batch_size, weights.shape[0])
+                kerns.append(nufft.calc_teoplitz_kernels(trj[None,], weights[b1:b2])[0])
+            L = temporal_funcs.shape[0]
+            self.toep_kerns = rearrange(torch.stack(kerns, dim=0), "(n1 n2) ... -> n1 n2 ...", n1=L, n2=L)
+        else:
+            self.toep_kerns = None
+
+    # ------------------------------------------------------------------
+    def forward(self, img: torch.Tensor) -> torch.Tensor:
+        """(*im_size) -> (C, *trj_size)."""
+        if self.plan is not None:
+            x = img.to(complex_dtype).contiguous()
+            ksp = torch.empty((self.mps.shape[0], *self.trj_size), dtype=complex_dtype, device=x.device)
+            self.plan.sense_forward(x, self.mps, ksp)
+            return ksp
+        L = self.spatial_funcs.shape[0]
+        nc = self.mps.shape[0]
+        ksp = torch.zeros((nc, *self.trj_size), dtype=complex_dtype, device=self.torch_dev)
+        sxb = self.mps * img
+        for l1, l2 in batch_iterator(L, L):
+            SBx = sxb[:, None, ...] * self.spatial_funcs[l1:l2]
+            FSBx = self.nufft.forward(SBx[None,], self.trj[None, ...])[0]
+            ksp += (FSBx * self.temporal_funcs[l1:l2]).sum(dim=-len(self.trj_size) - 1)
+        return ksp
+
+    def adjoint(self, ksp: torch.Tensor) -> torch.Tensor:
+        """(C, *trj_size) -> (*im_size)."""
+        if self.plan is not None:
+            y = ksp.to(complex_dtype).contiguous()
+            img = torch.empty(self.im_size, dtype=complex_dtype, device=y.device)
+            self.plan.sense_adjoint(y, self.dcf, self.mps, img)
+            return img
+        L = self.temporal_funcs.shape[0]
+        img = torch.zeros(self.im_size, dtype=complex_dtype, device=self.torch_dev)
+        kw = ksp * self.dcf[None, ...]
+        for l1, l2 in batch_iterator(L, L):
+            HWy = kw[:, None, ...] * self.temporal_funcs[l1:l2].conj()
+            FHWy = self.nufft.adjoint(HWy[None, ...], self.trj[None, ...])[0]
+            SFHWy = einsum(FHWy, self.mps.conj(), "nc nseg ..., nc ... -> nseg ...")
+            img += (SFHWy * self.spatial_funcs[l1:l2].conj()).sum(dim=-len(self.im_size) - 1)
+        return img
+
+    def normal(self, img: torch.Tensor) -> torch.Tensor:
+        """A^H A x (linops.py:1230-1308)."""
+        if not self.use_toeplitz:
+            if self.plan is not None:
+                x = img.to(complex_dtype).contiguous()
+                out = torch.empty_like(x)
+                self.plan.sense_normal(x, self.mps, self.dcf, out)
+                return out
+            return self.adjoint(self.forward(img))
+        L = self.temporal_funcs.shape[0]
+        dim = len(self.im_size)
+        im_size_os = self.toep_kerns.shape[-dim:]
+        padder = PadLast(im_size_os, self.im_size)
+        img_hat = torch.zeros_like(img)
+        kern = self.toep_kerns
+        Sx = self.mps * img
+        SBx = Sx[:, None, ...] * self.spatial_funcs  # C L *im
+        FSBx = fft(padder.forward(SBx), dim=tuple(range(-dim, 0)))
+        for m1, m2 in batch_iterator(L, 1 if dim == 3 else L):
+            MF = einsum(kern[m1:m2], FSBx, "M L ..., C L ... -> C M ...")
+            y = padder.adjoint(ifft(MF, dim=tuple(range(-dim, 0))))
+            y = (y * self.spatial_funcs[m1:m2].conj()).sum(dim=-dim - 1)
+            img_hat += (y * self.mps.conj()).sum(dim=0)
+        return img_hat

@@ -1,0 +1,372 @@
+"""GPU parity of the sm_100a NUFFT path against the reference's golden vectors
+(tests/golden, produced by the unmodified mr_recon) and against the CPU
+oracle on the same seeded inputs.
+
+Tolerances (relative L2): NUFFT forward/adjoint and split stages 1e-5
+(float32 arithmetic on both sides; measured ~1e-7..1e-6), gradients 1e-4,
+CG-SENSE 1e-4 against the float64-dot oracle CG."""
+
+import os
+import zlib
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import nufft_oracle as O
+from mr_recon_b200 import synth
+from mr_recon_b200.fourier import b200_nufft, triton_nufft
+from mr_recon_b200.interp import grid as mgrid, ungrid as mungrid
+from mr_recon_b200.plan import Plan
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda"
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+TOL = 1e-5
+
+
+def T(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(DEV)
+
+
+def Nn(t):
+    return t.detach().cpu().numpy()
+
+
+def rel(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def load(name):
+    return np.load(os.path.join(GOLD, name))
+
+
+# ----------------------------------------------------------------- golden
+def test_golden_radial_128_os2_w6():
+    g = load("nufft.npz")
+    nf = triton_nufft((128, 128), oversamp=2.0, width=6)
+    ksp = nf.forward(T(g["r128_img"]), T(g["r128_trj"]))
+    assert ksp.shape == g["r128_ksp"].shape
+    assert rel(Nn(ksp), g["r128_ksp"]) < TOL
+    adj = nf.adjoint(T(g["r128_ksp"]), T(g["r128_trj"]))
+    assert rel(Nn(adj), g["r128_adj"]) < TOL
+
+
+def test_golden_odd_sizes_odd_width_batched():
+    g = load("nufft.npz")
+    nf = b200_nufft((25, 22), oversamp=1.4, width=5)
+    assert rel(Nn(nf.forward(T(g["odd_img"]), T(g["odd_trj"]))), g["odd_ksp"]) < TOL
+    assert rel(Nn(nf.adjoint(T(g["odd_kin"]), T(g["odd_trj"]))), g["odd_adj"]) < TOL
+    assert rel(Nn(nf.forward_FT_only(T(g["odd_img"]))), g["odd_ft"]) < TOL
+
+
+def test_golden_3d_os125_w4():
+    g = load("nufft.npz")
+    nf = b200_nufft((16, 16, 16), oversamp=1.25, width=4)
+    assert rel(Nn(nf.forward(T(g["d3_img"]), T(g["d3_trj"]))), g["d3_ksp"]) < TOL
+    assert rel(Nn(nf.adjoint(T(g["d3_ksp"]), T(g["d3_trj"]))), g["d3_adj"]) < TOL
+
+
+def _interp_cases():
+    g = load("interp.npz")
+    keys = sorted(set(k.split("__")[0] for k in g.files))
+    return [(k, {f: g[k + "__" + f] for f in ["locs", "vals", "ungrid", "svals", "grid", "width", "beta", "gshape"]})
+            for k in keys]
+
+
+@pytest.mark.parametrize("case", _interp_cases(), ids=lambda c: c[0])
+def test_golden_ungrid_grid_with_edge_locations(case):
+    _, c = case
+    d = len(c["gshape"])
+    w = (int(c["width"]),) * d
+    kp = {"beta": float(c["beta"])}
+    u = mungrid(T(c["vals"]), T(c["locs"]), w, kernel_params=kp)
+    gg = mgrid(T(c["svals"]), T(c["locs"]), tuple(int(v) for v in c["gshape"]), w, kernel_params=kp)
+    assert rel(Nn(u), c["ungrid"]) < TOL
+    assert rel(Nn(gg), c["grid"]) < TOL
+
+
+def test_golden_image_gradient():
+    g = load("nufft.npz")
+    nf = b200_nufft((24, 24), oversamp=1.25, width=6)
+    x = T(g["ag_img"]).requires_grad_(True)
+    loss = (nf.forward(x, T(g["ag_trj"])) - T(g["ag_y"])).abs().square().sum()
+    loss.backward()
+    assert abs(loss.item() - float(g["ag_loss"])) / float(g["ag_loss"]) < 1e-5
+    assert rel(Nn(x.grad), g["ag_grad"]) < 1e-5
+
+
+def test_golden_toeplitz():
+    g = load("toeplitz.npz")
+    nf = b200_nufft((20, 20), oversamp=1.25, width=6)
+    k = nf.calc_teoplitz_kernels(T(g["trj"]), T(g["wts"]))
+    assert rel(Nn(k), g["kern"]) < 1e-5
+    assert rel(Nn(nf.normal_toeplitz(T(g["x"]), T(g["kern"]))), g["normal"]) < 1e-5
+
+
+def test_golden_sense_linop_and_cg():
+    from mr_recon_b200.linops import sense_linop
+    from mr_recon_b200.recons import CG_SENSE_recon
+    g = load("sense.npz")
+    nf = triton_nufft((32, 32), oversamp=1.25, width=6)
+    A = sense_linop(T(g["trj"]), T(g["mps"]), nufft=nf)
+    assert rel(Nn(A.adjoint(T(g["ksp"]))), g["adj"]) < TOL
+    assert rel(Nn(A.normal(T(g["truth"]))), g["normal"]) < TOL
+    rec = CG_SENSE_recon(A, T(g["ksp"]), max_iter=int(g["iters"]), lamda_l2=float(g["lamda"]),
+                         max_eigen=float(g["max_eigen"]), verbose=False)
+    # reference CG runs in float32; ours accumulates dots in float64
+    assert rel(Nn(rec), g["cg"]) < 3e-4
+    on = O.KBNufftOracle((32, 32), 1.25, 6)
+    ref64 = O.cg_sense(O.SenseOracle(g["trj"], g["mps"], on), g["ksp"], int(g["iters"]),
+                       float(g["lamda"]), float(g["max_eigen"]))
+    assert rel(Nn(rec), ref64) < 1e-4
+
+
+# ----------------------------------------------------------------- oracle parity
+CASES = [
+    # name, im_size, os, W, C, trajectory kind, M
+    ("2d_spiral_os125_w6", (96, 80), 1.25, 6, 5, "spiral", 6000),
+    ("2d_random_os2_w4_c1", (64, 64), 2.0, 4, 1, "random", 5000),
+    ("2d_radial_os2_w7_c3", (64, 48), 2.0, 7, 3, "radial", 4096),
+    ("3d_random_os125_w4", (20, 18, 22), 1.25, 4, 3, "random", 3000),
+    ("3d_koosh_os15_w5_c17", (16, 16, 16), 1.5, 5, 17, "koosh", 2048),
+    ("1d_random_os2_w6", (100,), 2.0, 6, 2, "random", 300),
+    ("2d_w10_os2", (40, 40), 2.0, 10, 2, "random", 800),
+]
+
+
+def _traj(kind, im, M, rng):
+    d = len(im)
+    if kind == "random":
+        return ((rng.rand(1, M, d) - 0.5) * np.array(im)).astype(np.float32)
+    if kind == "spiral":
+        n = 8
+        return synth.vd_spiral(n, M // n, min(im) / 2.0).reshape(1, -1, 2)
+    if kind == "radial":
+        n = 32
+        return synth.golden_angle_radial(n, M // n, min(im) / 2.0).reshape(1, -1, 2)
+    if kind == "koosh":
+        n = 64
+        return synth.kooshball(n, M // n, min(im) / 2.0).reshape(1, -1, 3)
+    raise ValueError(kind)
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: c[0])
+def test_oracle_parity_forward_adjoint_stages(case):
+    name, im, os_, W, C, kind, M = case
+    rng = np.random.RandomState(zlib.crc32(name.encode()) % (2 ** 31))
+    trj = _traj(kind, im, M, rng)
+    img = synth.randn_complex((1, C, *im), rng)
+    ksp_in = synth.randn_complex((1, C, trj.shape[1]), rng)
+    nf = b200_nufft(im, oversamp=os_, width=W)
+    on = O.KBNufftOracle(im, os_, W)
+    t = T(trj)
+    assert rel(Nn(nf.forward(T(img), t)), on.forward(img, trj)) < TOL
+    assert rel(Nn(nf.adjoint(T(ksp_in), t)), on.adjoint(ksp_in, trj)) < TOL
+    ft = nf.forward_FT_only(T(img))
+    assert rel(Nn(ft), on.forward_FT_only(img)) < TOL
+    assert rel(Nn(nf.forward_interp_only(ft, t)), on.forward_interp_only(on.forward_FT_only(img), trj)) < TOL
+    g = nf.adjoint_grid_only(T(ksp_in), t)
+    assert rel(Nn(g), on.adjoint_grid_only(ksp_in, trj)) < TOL
+    assert rel(Nn(nf.adjoint_iFT_only(g)), on.adjoint_iFT_only(on.adjoint_grid_only(ksp_in, trj))) < TOL
+
+
+def test_split_heavy_tiles_match_oracle():
+    """A dense cluster of samples with a tiny work-item size forces tiles to be
+    split over many CTAs (zero pre-pass + atomic write-back in gridding)."""
+    rng = np.random.RandomState(7)
+    im = (48, 48)
+    trj = np.concatenate([(rng.rand(1, 4000, 2) - 0.5) * 3.0, (rng.rand(1, 1000, 2) - 0.5) * 48], 1).astype(np.float32)
+    img = synth.randn_complex((1, 4, *im), rng)
+    y = synth.randn_complex((1, 4, trj.shape[1]), rng)
+    nf = b200_nufft(im, oversamp=1.25, width=6, max_chunk=64)
+    on = O.KBNufftOracle(im, 1.25, 6)
+    assert rel(Nn(nf.forward(T(img), T(trj))), on.forward(img, trj)) < TOL
+    assert rel(Nn(nf.adjoint(T(y), T(trj))), on.adjoint(y, trj)) < TOL
+    plan = nf._plans.entries[-1][2]
+    assert plan.stats()["split_tiles"] > 0
+
+
+@pytest.mark.parametrize("tile", [(8, 8), (16, 32), (64, 64), (5, 7)])
+def test_tile_shapes_agree(tile):
+    rng = np.random.RandomState(11)
+    im = (64, 72)
+    trj = synth.vd_spiral(6, 700, 32.0).reshape(1, -1, 2)
+    img = synth.randn_complex((1, 9, *im), rng)
+    y = synth.randn_complex((1, 9, trj.shape[1]), rng)
+    on = O.KBNufftOracle(im, 1.25, 6)
+    nf = b200_nufft(im, oversamp=1.25, width=6, tile=tile, coil_group=4)
+    assert rel(Nn(nf.forward(T(img), T(trj))), on.forward(img, trj)) < TOL
+    assert rel(Nn(nf.adjoint(T(y), T(trj))), on.adjoint(y, trj)) < TOL
+
+
+def test_edge_cases():
+    rng = np.random.RandomState(3)
+    im = (32, 32)
+    nf = b200_nufft(im, oversamp=1.25, width=6)
+    on = O.KBNufftOracle(im, 1.25, 6)
+    # exact grid points, exact kernel edges, k = -N/2, far out of range (wraps)
+    pts = np.array([[0, 0], [-16, -16], [15.999, 15.999], [1.0, -2.0], [3.2, 0.0],
+                    [40.0, -50.25], [-0.0, 7.5], [0.4, 0.4]], dtype=np.float32)[None]
+    img = synth.randn_complex((1, 2, *im), rng)
+    assert rel(Nn(nf.forward(T(img), T(pts))), on.forward(img, pts)) < TOL
+    y = synth.randn_complex((1, 2, pts.shape[1]), rng)
+    assert rel(Nn(nf.adjoint(T(y), T(pts))), on.adjoint(y, pts)) < TOL
+    # a single sample, a single coil
+    one = pts[:, :1]
+    assert rel(Nn(nf.forward(T(img[:, :1]), T(one))), on.forward(img[:, :1], one)) < TOL
+    # empty trajectory: adjoint is zero, forward is empty
+    empty = np.zeros((1, 0, 2), np.float32)
+    assert nf.forward(T(img), T(empty)).shape == (1, 2, 0)
+    assert float(nf.adjoint(T(np.zeros((1, 2, 0), np.complex64)), T(empty)).abs().max()) == 0.0
+    # grid smaller than the kernel (raw interpolation wraps several times)
+    vals = synth.randn_complex((3, 4, 5), rng)
+    locs = (rng.rand(50, 2) * 10 - 3).astype(np.float32)
+    u = mungrid(T(vals), T(locs), (6, 6), kernel_params={"beta": 9.0})
+    assert rel(Nn(u), O.ungrid(vals, locs, (6, 6), 9.0)) < TOL
+    gg = mgrid(T(synth.randn_complex((3, 50), rng)), T(locs), (4, 5), (6, 6), kernel_params={"beta": 9.0})
+    assert gg.shape == (3, 4, 5)
+
+
+def test_errors_match_reference_behaviour():
+    nf = b200_nufft((16, 16))
+    with pytest.raises(RuntimeError):
+        nf.forward(torch.zeros(1, 1, 16, 16, dtype=torch.complex64), torch.zeros(1, 4, 2))
+    with pytest.raises(ValueError):
+        mungrid(torch.zeros(1, 8, 8, dtype=torch.complex64, device=DEV), torch.zeros(3, 2, device=DEV), (20, 20))
+    with pytest.raises(NotImplementedError):
+        mungrid(torch.zeros(1, 8, 8, dtype=torch.complex64, device=DEV), torch.zeros(3, 2, device=DEV), (4, 4),
+                kernel="spline")
+
+
+# ----------------------------------------------------------------- properties at full size
+def test_adjoint_consistency_and_linearity_config2_size():
+    """<A x, y> = <x, A^H y> and A(a x1 + x2) = a A x1 + A x2 on the 256^2,
+    32-coil, 48 x 2048 spiral geometry."""
+    rng = np.random.RandomState(5)
+    im = (256, 256)
+    trj = T(synth.vd_spiral(48, 2048, 128.0)[None])
+    x1 = torch.randn(1, 32, *im, dtype=torch.complex64, device=DEV)
+    x2 = torch.randn(1, 32, *im, dtype=torch.complex64, device=DEV)
+    y = torch.randn(1, 32, 48, 2048, dtype=torch.complex64, device=DEV)
+    nf = b200_nufft(im)
+    Ax = nf.forward(x1, trj)
+    AHy = nf.adjoint(y, trj)
+    lhs = torch.vdot(Ax.reshape(-1).to(torch.complex128), y.reshape(-1).to(torch.complex128))
+    rhs = torch.vdot(x1.reshape(-1).to(torch.complex128), AHy.reshape(-1).to(torch.complex128))
+    assert abs(lhs - rhs) / abs(lhs) < 1e-5
+    a = 0.7 - 0.2j
+    lin = nf.forward(a * x1 + x2, trj)
+    ref = a * Ax + nf.forward(x2, trj)
+    assert float((lin - ref).abs().norm() / ref.abs().norm()) < 1e-5
+    del rng
+
+
+# ----------------------------------------------------------------- trajectory gradients
+@pytest.mark.parametrize("d", [2, 3])
+def test_trajectory_gradient_forward_vs_fp64_finite_differences(d):
+    rng = np.random.RandomState(20 + d)
+    im = (24, 20) if d == 2 else (12, 10, 14)
+    W = 6 if d == 2 else 4
+    os_ = 1.25
+    M = 400
+    trj = ((rng.rand(1, M, d) - 0.5) * np.array(im)).astype(np.float32)
+    img = synth.randn_complex((1, 3, *im), rng)
+    y = synth.randn_complex((1, 3, M), rng)
+    nf = b200_nufft(im, oversamp=os_, width=W)
+    t = T(trj).requires_grad_(True)
+    loss = torch.sum(torch.view_as_real(nf.forward(T(img), t)) * torch.view_as_real(T(y)))
+    loss.backward()
+    g = Nn(t.grad)
+    h = 1e-5
+    idx = rng.choice(M, 12, replace=False)
+    fds, ans = [], []
+    for p in idx:
+        for ax in range(d):
+            tp = trj.astype(np.float64).copy()
+            tm = tp.copy()
+            tp[0, p, ax] += h
+            tm[0, p, ax] -= h
+            fp = np.sum(np.real(np.conj(y) * O.nufft_forward_f64(img, tp, im, os_, W, nf.beta)))
+            fm = np.sum(np.real(np.conj(y) * O.nufft_forward_f64(img, tm, im, os_, W, nf.beta)))
+            fds.append((fp - fm) / (2 * h))
+            ans.append(g[0, p, ax])
+    assert rel(ans, fds) < 1e-4
+
+
+def test_trajectory_gradient_adjoint_and_interp_vs_fp64_fd():
+    """Trajectory gradient through the adjoint NUFFT: d/dk Re<z, A^H(y; k)>
+    equals d/dk Re<A(z; k), y>, checked by float64 central differences."""
+    rng = np.random.RandomState(31)
+    im = (20, 20)
+    M = 300
+    trj = ((rng.rand(1, M, 2) - 0.5) * 20).astype(np.float32)
+    z = synth.randn_complex((1, 2, *im), rng)
+    y = synth.randn_complex((1, 2, M), rng)
+    nf = b200_nufft(im, oversamp=1.25, width=6)
+    t = T(trj).requires_grad_(True)
+    loss = torch.sum(torch.view_as_real(nf.adjoint(T(y), t)) * torch.view_as_real(T(z)))
+    loss.backward()
+    g = Nn(t.grad)
+    h = 1e-5
+    fds, ans = [], []
+    for p in rng.choice(M, 10, replace=False):
+        for ax in range(2):
+            tp = trj.astype(np.float64).copy()
+            tm = tp.copy()
+            tp[0, p, ax] += h
+            tm[0, p, ax] -= h
+            fp = np.sum(np.real(np.conj(O.nufft_forward_f64(z, tp, im, 1.25, 6, nf.beta)) * y))
+            fm = np.sum(np.real(np.conj(O.nufft_forward_f64(z, tm, im, 1.25, 6, nf.beta)) * y))
+            fds.append((fp - fm) / (2 * h))
+            ans.append(g[0, p, ax])
+    assert rel(ans, fds) < 1e-4
+
+
+# ----------------------------------------------------------------- uneven batches
+def test_uneven_multislice_plan_matches_per_slice_oracle():
+    rng = np.random.RandomState(9)
+    sizes = [(40, 40), (48, 32), (40, 40), (56, 56)]
+    coils = [3, 1, 5, 2]
+    npts = [900, 400, 1300, 700]
+    plan = Plan(sizes, npts, coils, 1.25, (6.0, 6.0), device=DEV)
+    trjs = [((rng.rand(m, 2) - 0.5) * np.array(s)).astype(np.float32) for s, m in zip(sizes, npts)]
+    imgs = [synth.randn_complex((c, *s), rng) for s, c in zip(sizes, coils)]
+    plan.set_traj(T(np.concatenate([t.reshape(-1) for t in trjs])))
+    img_flat = T(np.concatenate([i.reshape(-1) for i in imgs]))
+    ksp = torch.empty(plan.n_ksp, dtype=torch.complex64, device=DEV)
+    plan.forward(img_flat, ksp)
+    back = torch.empty(plan.n_img, dtype=torch.complex64, device=DEV)
+    plan.adjoint(ksp, back)
+    k = Nn(ksp)
+    b = Nn(back)
+    for s in range(4):
+        on = O.KBNufftOracle(sizes[s], 1.25, 6)
+        kr = on.forward(imgs[s][None], trjs[s][None])[0]
+        ko = k[plan.ksp_off[s]:plan.ksp_off[s] + coils[s] * npts[s]].reshape(kr.shape)
+        assert rel(ko, kr) < TOL
+        br = on.adjoint(ko[None], trjs[s][None])[0]
+        bo = b[plan.img_off[s]:plan.img_off[s] + br.size].reshape(br.shape)
+        assert rel(bo, br) < TOL
+
+
+def test_sense_cg_graph_matches_oracle():
+    from mr_recon_b200.linops import sense_linop
+    from mr_recon_b200.recons import CG_SENSE_recon
+    rng = np.random.RandomState(12)
+    im = (48, 48)
+    C = 6
+    mps = synth.gaussian_coil_maps(im, C)
+    trj = synth.vd_spiral(6, 500, 24.0)
+    truth = synth.ellipse_phantom(im, 8, rng)
+    on = O.KBNufftOracle(im, 1.25, 6)
+    Ao = O.SenseOracle(trj, mps, on)
+    ksp = synth.add_noise(Ao.forward(truth), 30.0, rng)
+    ref = O.cg_sense(Ao, ksp, 8, 1e-3, 1.5)
+    A = sense_linop(T(trj), T(mps), nufft=b200_nufft(im))
+    x_eager = CG_SENSE_recon(A, T(ksp), max_iter=8, lamda_l2=1e-3, max_eigen=1.5, verbose=False)
+    x_graph = CG_SENSE_recon(A, T(ksp), max_iter=8, lamda_l2=1e-3, max_eigen=1.5, verbose=False, graph=True)
+    assert rel(Nn(x_eager), ref) < 1e-4
+    assert rel(Nn(x_graph), ref) < 1e-4
