@@ -83,6 +83,13 @@ int mrn_plan_sizes(const mrn_plan* plan, int64_t* out8);
  * gridding entries, and split (multi-item) gridding tiles, in out4. */
 int mrn_plan_stats(mrn_plan* plan, int64_t* out4);
 
+/* Plan options (no counterpart in the reference).
+ * MRN_OPT_FAST_KERNELS (default 1): use the unrolled fixed-width tile kernels
+ * where they apply (2D/3D, equal width in [4, 8) per dimension); 0 forces the
+ * general kernels. Both compute the same taps and weights. */
+#define MRN_OPT_FAST_KERNELS 1
+int mrn_plan_set_option(mrn_plan* plan, int option, int value);
+
 /* Stage timing, a profiling aid with no counterpart in the reference (which
  * only prints wall-clock, recons.py:127-133). When on, every call records a
  * CUDA event pair around each stage on the launching stream (not for use

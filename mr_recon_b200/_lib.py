@@ -26,6 +26,7 @@ MRN_ERR_UNSUPPORTED = -7
 
 MRN_PLAN_RAW = 1
 MRN_PLAN_NO_APOD = 2
+MRN_OPT_FAST_KERNELS = 1
 
 _vp = C.c_void_p
 _i = C.c_int
@@ -46,6 +47,7 @@ SIGNATURES = {
     "mrn_plan_offsets": (_i, [_vp, _pi64, _pi64, _pi64, _pi64]),
     "mrn_plan_sizes": (_i, [_vp, _pi64]),
     "mrn_plan_stats": (_i, [_vp, _pi64]),
+    "mrn_plan_set_option": (_i, [_vp, _i, _i]),
     "mrn_plan_enable_timing": (_i, [_vp, _i]),
     "mrn_plan_timing": (_i, [_vp, _pd, _pi64]),
     "mrn_plan_set_traj": (_i, [_vp, _vp, _vp]),

@@ -156,6 +156,7 @@ struct mrn_plan {
   int max_coil = 1;
   int max_chunk = 1024;
   int tap_max = 8;  // compile-time tap bound used (8 or 16)
+  bool use_fast = true;  // use the unrolled fixed-K tile kernels where they apply
   mrn::KBParams kb{};
   std::vector<mrn::SliceGeom> h_slices;
   int64_t n_img = 0, n_ksp = 0, n_grid = 0, n_trj = 0, n_pts = 0, n_x = 0;

@@ -21,6 +21,15 @@ int launch_grid_t(mrn_plan* P, const float2* ksp, const float* dcf, const float2
 int launch_traj_grad(mrn_plan* P, const float2* grid, GridLayout layout, const float2* samples,
                      float* out, float scale, cudaStream_t st);
 
+// Fast paths with compile-time tap counts (tiles_fast.cu)
+bool fast_path_ok(const mrn_plan* P, bool gridding);
+int launch_interp_fast(mrn_plan* P, const float2* grid, int layout, float2* ksp, float scale,
+                       const float2* temporal, int cg, int G, int pstride, size_t smem, dim3 gdim,
+                       cudaStream_t st);
+int launch_grid_fast(mrn_plan* P, const float2* ksp, const float* dcf, const float2* temporal,
+                     int layout, float2* grid, float scale, int cg, int G, int pstride, size_t smem,
+                     dim3 gdim, cudaStream_t st);
+
 // FFT-stage kernels (fftstage.cu)
 enum PreMode { kPrePlain = 0, kPreSense = 1 };
 int launch_pre(mrn_plan* P, PreMode mode, const float2* src, const float2* mps, float scale,

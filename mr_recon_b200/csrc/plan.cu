@@ -509,6 +509,14 @@ int mrn_plan_create(mrn_plan** out, int ndim, int n_slices, const int* im_size,
   return MRN_OK;
 }
 
+int mrn_plan_set_option(mrn_plan* P, int option, int value) {
+  if (!P) return MRN_ERR_ARG;
+  switch (option) {
+    case MRN_OPT_FAST_KERNELS: P->use_fast = value != 0; return MRN_OK;
+    default: return MRN_ERR_ARG;
+  }
+}
+
 int mrn_plan_enable_timing(mrn_plan* P, int on) {
   if (!P) return MRN_ERR_ARG;
   P->timing = on != 0;

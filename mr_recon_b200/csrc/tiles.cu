@@ -470,12 +470,13 @@ __global__ void k_zero_split(const int* __restrict__ split_tiles, const int* __r
   for (int i = 0; i < kMaxDim; ++i) hs[i] = (i < D && layout == kInternal) ? g.hshift[i] : 0;
   int cells = 1;
   for (int i = 0; i < D; ++i) cells *= f.size[i];
-  const int64_t goff = layout == kInternal ? g.grid_off : g.ugrid_off;
-  for (int idx = threadIdx.x; idx < cells * g.ncoil; idx += blockDim.x) {
-    const int c = idx / cells, cell = idx - c * cells;
+  const int c = blockIdx.y;  // one CTA per (split tile, coil)
+  if (c >= g.ncoil) return;
+  const int64_t goff = (layout == kInternal ? g.grid_off : g.ugrid_off) + (int64_t)c * g.gos;
+  for (int cell = threadIdx.x; cell < cells; cell += blockDim.x) {
     int64_t lin;
     tile_storage<D>(g, f, hs, cell, &lin);
-    grid[goff + (int64_t)c * g.gos + lin] = make_float2(0.f, 0.f);
+    grid[goff + lin] = make_float2(0.f, 0.f);
   }
 }
 
@@ -668,7 +669,7 @@ struct Layout {
 };
 
 // Shared-memory layout for one kernel kind: 0 interp, 1 grid, 2 traj grad.
-static Layout plan_layout(const mrn_plan* P, int kind) {
+static Layout plan_layout(const mrn_plan* P, int kind, bool fast = false) {
   const int D = P->ndim;
   int64_t cells = 1;
   for (int i = 0; i < D; ++i)
@@ -681,7 +682,7 @@ static Layout plan_layout(const mrn_plan* P, int kind) {
     const int G = pick_g(cg);
     const int slots = 32 / G;
     size_t per_warp = (size_t)D * KM * slots * 4;
-    size_t fixed = kWarps * per_warp * (kind == 0 ? 1 : 2);
+    size_t fixed = fast ? 0 : kWarps * per_warp * (kind == 0 ? 1 : 2);
     size_t data = (size_t)cg * pstride * 8;
     size_t total = fixed + data;
     if (total <= kSmemMax || cg == 1) {
@@ -728,9 +729,13 @@ static int prepare(K kernel, size_t smem) {
 int launch_interp(mrn_plan* P, const float2* grid, GridLayout layout, float2* ksp, float scale,
                   const float2* temporal, cudaStream_t st) {
   if (P->n_items_interp == 0) return MRN_OK;
-  const Layout L = plan_layout(P, 0);
+  const bool fast = P->use_fast && fast_path_ok(P, false);
+  const Layout L = plan_layout(P, 0, fast);
   const int G = pick_g(L.cg);
   dim3 gridDim((unsigned)P->n_items_interp, (unsigned)((P->max_coil + L.cg - 1) / L.cg));
+  if (fast)
+    return launch_interp_fast(P, grid, (int)layout, ksp, scale, temporal, L.cg, G, L.pstride, L.smem,
+                              gridDim, st);
   int rc = MRN_OK;
   MRN_DISPATCH_DK(P->ndim, P->tap_max, MRN_DISPATCH_G(G, {
     auto kern = k_interp<DD, GG, KK>;
@@ -753,10 +758,11 @@ int launch_grid(mrn_plan* P, const float2* ksp, const float* dcf, GridLayout lay
 int launch_grid_t(mrn_plan* P, const float2* ksp, const float* dcf, const float2* temporal,
                   GridLayout layout, float2* grid, float scale, cudaStream_t st) {
   if (P->n_items_grid == 0) return MRN_OK;
-  const Layout L = plan_layout(P, 1);
+  const bool fast = P->use_fast && fast_path_ok(P, true);
+  const Layout L = plan_layout(P, 1, fast);
   const int G = pick_g(L.cg);
   if (P->n_split > 0) {
-    const unsigned nb = (unsigned)P->n_split;
+    const dim3 nb((unsigned)P->n_split, (unsigned)P->max_coil);
     if (P->ndim == 1)
       k_zero_split<1><<<nb, 256, 0, st>>>(P->d_split_tiles, P->d_counts, P->d_slices, P->nslices, grid, (int)layout);
     else if (P->ndim == 2)
@@ -765,6 +771,9 @@ int launch_grid_t(mrn_plan* P, const float2* ksp, const float* dcf, const float2
       k_zero_split<3><<<nb, 256, 0, st>>>(P->d_split_tiles, P->d_counts, P->d_slices, P->nslices, grid, (int)layout);
   }
   dim3 gridDim((unsigned)P->n_items_grid, (unsigned)((P->max_coil + L.cg - 1) / L.cg));
+  if (fast)
+    return launch_grid_fast(P, ksp, dcf, temporal, (int)layout, grid, scale, L.cg, G, L.pstride, L.smem,
+                            gridDim, st);
   int rc = MRN_OK;
   MRN_DISPATCH_DK(P->ndim, P->tap_max, MRN_DISPATCH_G(G, {
     auto kern = k_grid<DD, GG, KK>;

@@ -1,0 +1,494 @@
+// Fast paths of the tile kernels for the common kernel widths: the number of
+// candidate taps per dimension K = floor(W) + 1 is a compile-time constant,
+// so the K^d tap loop is fully unrolled with immediate shared-memory offsets.
+//
+// Same algorithm and numerics as tiles.cu (tap j = lo + q, lo = ceil(u - W/2),
+// valid iff |(float)j - u| <= W/2, separable KB weights, circular cells);
+// the differences are in the instruction stream only:
+//   * the d*K 1D weights of a sample are computed once by the G lanes that
+//     share it (one weight per lane) and broadcast with warp shuffles;
+//   * an invalid tap (outside the kernel support, or, for gridding, outside
+//     the tile this CTA owns) gets weight 0 and is skipped by a predicate,
+//     so there is no data-dependent loop bound;
+//   * no integer division in the per-sample path.
+// Used when every dimension has the same K in {5,6,7,8} (W in [4, 8)) and
+// d in {2, 3}; gridding additionally needs >= 2 tiles per dimension (so a
+// footprint meets a tile in one contiguous run).
+#include <algorithm>
+
+#include "common.cuh"
+#include "internal.cuh"
+
+namespace mrn {
+
+namespace {
+
+struct Frame {
+  int org[kMaxDim];
+  int size[kMaxDim];
+};
+
+__device__ __forceinline__ Frame frame_of(const SliceGeom& g, int tile, int D) {
+  Frame f;
+  int rem = tile;
+  int tc[kMaxDim] = {0, 0, 0};
+  for (int i = D - 1; i >= 0; --i) {
+    tc[i] = rem % g.ntile[i];
+    rem /= g.ntile[i];
+  }
+#pragma unroll
+  for (int i = 0; i < kMaxDim; ++i) {
+    if (i < D) {
+      f.org[i] = tile_begin(tc[i], g.nos[i], g.ntile[i]);
+      f.size[i] = tile_begin(tc[i] + 1, g.nos[i], g.ntile[i]) - f.org[i];
+    } else {
+      f.org[i] = 0;
+      f.size[i] = 1;
+    }
+  }
+  return f;
+}
+
+__device__ __forceinline__ int wrap_once(int a, int n) {
+  // a in (-n, 2n): a mod n
+  a = a < 0 ? a + n : a;
+  return a >= n ? a - n : a;
+}
+
+__device__ __forceinline__ float sel3(const float* v, int i) { return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]); }
+__device__ __forceinline__ int sel3i(const int* v, int i) { return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]); }
+
+// 1D weights of one sample, w[i][q] for dim i, tap q (0 when invalid). The G
+// lanes of a slot compute D*K entries round-robin and exchange them by shuffles.
+template <int D, int K, int G>
+__device__ __forceinline__ void sample_weights(const float* u, const int* lo, const float* r,
+                                               float beta, int lane, float (&w)[D][K]) {
+  constexpr int NW = D * K;
+  constexpr int IT = (NW + G - 1) / G;
+  const int lg = lane % G;
+  float mine[IT];
+#pragma unroll
+  for (int it = 0; it < IT; ++it) {
+    const int t = it * G + lg;
+    float v = 0.f;
+    if (t < NW) {
+      const int i = t / K;
+      const int q = t - i * K;
+      const float ui = sel3(u, i), ri = sel3(r, i);
+      const float adx = fabsf(__fsub_rn((float)(sel3i(lo, i) + q), ui));
+      if (adx <= ri) v = kb_tap(adx, ri, beta);
+    }
+    mine[it] = v;
+  }
+  if (G == 1) {
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int q = 0; q < K; ++q) w[i][q] = mine[i * K + q];
+  } else {
+    const int base = lane - lg;
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int q = 0; q < K; ++q) {
+        const int t = i * K + q;
+        w[i][q] = __shfl_sync(0xffffffffu, mine[t / G], base + (t % G));
+      }
+  }
+}
+
+// Region loader (tile + halo, wrapped), one warp per row -- as tiles.cu.
+template <int D>
+__device__ __forceinline__ void load_region_f(float2* __restrict__ tile, const float2* __restrict__ grid,
+                                              int64_t goff, int64_t gos, const int* nos,
+                                              const int* org, const int* ext, const int* hs, int ncg,
+                                              int pstride) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int inner = ext[D - 1];
+  int outer = 1;
+#pragma unroll
+  for (int i = 0; i < D - 1; ++i) outer *= ext[i];
+  const int nrows = ncg * outer;
+  const int nl = nos[D - 1];
+  // storage index of local column 0 and the local column where it wraps
+  const int s_first = wrap_once(org[D - 1] - hs[D - 1], nl);
+  for (int row = warp; row < nrows; row += kWarps) {
+    const int c = row / outer;
+    int rr = row - c * outer;
+    int l[kMaxDim] = {0, 0, 0};
+#pragma unroll
+    for (int i = D - 2; i >= 0; --i) {
+      l[i] = rr % ext[i];
+      rr /= ext[i];
+    }
+    int64_t base = 0;
+    int lbase = 0;
+#pragma unroll
+    for (int i = 0; i < D - 1; ++i) {
+      base = base * nos[i] + wrap_once(org[i] + l[i] - hs[i], nos[i]);
+      lbase = lbase * ext[i] + l[i];
+    }
+    const float2* src = grid + goff + (int64_t)c * gos + base * nl;
+    float2* dst = tile + c * pstride + lbase * inner;
+    for (int q = lane; q < inner; q += 32) {
+      int s = s_first + q;
+      while (s >= nl) s -= nl;
+      dst[q] = __ldg(src + s);
+    }
+  }
+}
+
+}  // namespace
+
+template <int D, int K, int G>
+__global__ void __launch_bounds__(kThreads)
+k_interp_fast(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBParams kb,
+              const float4* __restrict__ coord, const int* __restrict__ perm,
+              const float2* __restrict__ grid, int layout, float2* __restrict__ ksp, float scale,
+              const float2* __restrict__ temporal, int cg, int pstride) {
+  constexpr int SLOTS = 32 / G;
+  constexpr int CPL = G == 32 ? 2 : 1;
+  extern __shared__ float4 smem_f4[];
+  float2* tile = reinterpret_cast<float2*>(smem_f4);
+
+  const Item it = items[blockIdx.x];
+  const SliceGeom* gp = sl + it.slice;
+  const int ncoil = gp->ncoil;
+  const int c0 = blockIdx.y * cg;
+  if (c0 >= ncoil) return;
+  const int ncg = min(cg, ncoil - c0);
+  int nos[kMaxDim], hs[kMaxDim], ext[kMaxDim];
+#pragma unroll
+  for (int i = 0; i < kMaxDim; ++i) {
+    nos[i] = gp->nos[i];
+    hs[i] = (i < D && layout == kInternal) ? gp->hshift[i] : 0;
+  }
+  const Frame f = frame_of(*gp, it.tile, D);
+#pragma unroll
+  for (int i = 0; i < kMaxDim; ++i) ext[i] = i < D ? f.size[i] + K - 1 : 1;
+  const int64_t gos = gp->gos;
+  const int64_t goff = (layout == kInternal ? gp->grid_off : gp->ugrid_off) + (int64_t)c0 * gos;
+  const int64_t m = gp->m, pt_off = gp->pt_off, ksp_off = gp->ksp_off;
+  load_region_f<D>(tile, grid, goff, gos, nos, f.org, ext, hs, ncg, pstride);
+  __syncthreads();
+
+  const float r[3] = {kb.radius[0], kb.radius[1], kb.radius[2]};
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int slot = lane / G, lg = lane % G;
+  for (int base = warp * SLOTS; base < it.count; base += kWarps * SLOTS) {
+    const int el = base + slot;
+    const bool active = el < it.count;
+    const int e = it.start + (active ? el : 0);
+    const float4 c4 = coord[e];
+    const float u[3] = {c4.x, c4.y, c4.z};
+    int lo[3] = {0, 0, 0}, l0[3] = {0, 0, 0};
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      lo[i] = (int)ceilf(__fsub_rn(u[i], r[i]));
+      l0[i] = wrap_once(lo[i], nos[i]) - f.org[i];
+    }
+    float w[D][K];
+    sample_weights<D, K, G>(u, lo, r, kb.beta, lane, w);
+    if (!active) continue;
+    const int64_t lp = perm[e] - pt_off;
+    float2 h = make_float2(scale, 0.f);
+    if (temporal) {
+      const float2 t = temporal[pt_off + lp];
+      h = make_float2(scale * t.x, scale * t.y);
+    }
+#pragma unroll
+    for (int q = 0; q < CPL; ++q) {
+      const int c = lg + q * G;
+      if (c >= ncg) break;
+      const float2* tb = tile + c * pstride;
+      float ax = 0.f, ay = 0.f;
+      if (D == 2) {
+#pragma unroll
+        for (int a = 0; a < K; ++a) {
+          const float wa = w[0][a];
+          if (wa == 0.f) continue;
+          const float2* rp = tb + (l0[0] + a) * ext[1] + l0[1];
+#pragma unroll
+          for (int b = 0; b < K; ++b) {
+            const float ww = wa * w[D - 1][b];
+            const float2 v = rp[b];
+            ax = fmaf(ww, v.x, ax);
+            ay = fmaf(ww, v.y, ay);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int a = 0; a < K; ++a) {
+          const float wa = w[0][a];
+          if (wa == 0.f) continue;
+#pragma unroll
+          for (int b = 0; b < K; ++b) {
+            const float wab = wa * w[D > 2 ? 1 : 0][b];
+            if (wab == 0.f) continue;
+            const float2* rp = tb + ((l0[0] + a) * ext[1] + (l0[1] + b)) * ext[2] + l0[2];
+#pragma unroll
+            for (int z = 0; z < K; ++z) {
+              const float ww = wab * w[D - 1][z];
+              const float2 v = rp[z];
+              ax = fmaf(ww, v.x, ax);
+              ay = fmaf(ww, v.y, ay);
+            }
+          }
+        }
+      }
+      float2* dst = ksp + ksp_off + (int64_t)(c0 + c) * m + lp;
+      const float2 v = make_float2(ax * h.x - ay * h.y, ax * h.y + ay * h.x);
+      if (temporal) {
+        const float2 o = *dst;
+        *dst = make_float2(o.x + v.x, o.y + v.y);
+      } else {
+        *dst = v;
+      }
+    }
+  }
+}
+
+template <int D, int K, int G>
+__global__ void __launch_bounds__(kThreads)
+k_grid_fast(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBParams kb,
+            const float4* __restrict__ coord, const int* __restrict__ perm,
+            const float2* __restrict__ ksp, const float* __restrict__ dcf,
+            const float2* __restrict__ temporal, float2* __restrict__ grid, int layout, float scale,
+            int cg, int pstride) {
+  constexpr int SLOTS = 32 / G;
+  constexpr int CPL = G == 32 ? 2 : 1;
+  extern __shared__ float4 smem_f4[];
+  float* acc_re = reinterpret_cast<float*>(smem_f4);
+  float* acc_im = acc_re + (size_t)cg * pstride;
+
+  const Item it = items[blockIdx.x];
+  const SliceGeom* gp = sl + it.slice;
+  const int ncoil = gp->ncoil;
+  const int c0 = blockIdx.y * cg;
+  if (c0 >= ncoil) return;
+  const int ncg = min(cg, ncoil - c0);
+  int nos[kMaxDim], hs[kMaxDim];
+#pragma unroll
+  for (int i = 0; i < kMaxDim; ++i) {
+    nos[i] = gp->nos[i];
+    hs[i] = (i < D && layout == kInternal) ? gp->hshift[i] : 0;
+  }
+  const Frame f = frame_of(*gp, it.tile, D);
+  int cells = 1;
+#pragma unroll
+  for (int i = 0; i < D; ++i) cells *= f.size[i];
+  for (int idx = threadIdx.x; idx < ncg * pstride; idx += kThreads) {
+    acc_re[idx] = 0.f;
+    acc_im[idx] = 0.f;
+  }
+  __syncthreads();
+
+  const int64_t m = gp->m, pt_off = gp->pt_off, ksp_off = gp->ksp_off;
+  const float r[3] = {kb.radius[0], kb.radius[1], kb.radius[2]};
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int slot = lane / G, lg = lane % G;
+  for (int base = warp * SLOTS; base < it.count; base += kWarps * SLOTS) {
+    const int el = base + slot;
+    const bool active = el < it.count;
+    const int e = it.start + (active ? el : 0);
+    const float4 c4 = coord[e];
+    const float u[3] = {c4.x, c4.y, c4.z};
+    int lo[3] = {0, 0, 0}, st[3] = {0, 0, 0};
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      lo[i] = (int)ceilf(__fsub_rn(u[i], r[i]));
+      int s = wrap_once(lo[i], nos[i]) - f.org[i];
+      if (s >= f.size[i]) s -= nos[i];  // footprint wraps into this tile from the end
+      st[i] = s;
+    }
+    float w[D][K];
+    sample_weights<D, K, G>(u, lo, r, kb.beta, lane, w);
+    // taps outside the owned tile get weight 0
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int q = 0; q < K; ++q) {
+        const int l = st[i] + q;
+        if (l < 0 || l >= f.size[i]) w[i][q] = 0.f;
+      }
+    if (!active) continue;
+    const int64_t lp = perm[e] - pt_off;
+    float vs = scale;
+    if (dcf) vs *= dcf[pt_off + lp];
+    float2 h = make_float2(vs, 0.f);
+    if (temporal) {
+      const float2 t = temporal[pt_off + lp];
+      h = make_float2(vs * t.x, -vs * t.y);
+    }
+#pragma unroll
+    for (int q = 0; q < CPL; ++q) {
+      const int c = lg + q * G;
+      if (c >= ncg) break;
+      const float2 a0 = __ldg(ksp + ksp_off + (int64_t)(c0 + c) * m + lp);
+      const float2 v = make_float2(a0.x * h.x - a0.y * h.y, a0.x * h.y + a0.y * h.x);
+      float* re = acc_re + c * pstride;
+      float* im = acc_im + c * pstride;
+      if (D == 2) {
+#pragma unroll
+        for (int a = 0; a < K; ++a) {
+          const float wa = w[0][a];
+          if (wa == 0.f) continue;
+          const int row = (st[0] + a) * f.size[1] + st[1];
+          const float vx = wa * v.x, vy = wa * v.y;
+#pragma unroll
+          for (int b = 0; b < K; ++b) {
+            const float wb = w[1][b];
+            if (wb != 0.f) {
+              atomicAdd(re + row + b, wb * vx);
+              atomicAdd(im + row + b, wb * vy);
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int a = 0; a < K; ++a) {
+          const float wa = w[0][a];
+          if (wa == 0.f) continue;
+#pragma unroll
+          for (int b = 0; b < K; ++b) {
+            const float wab = wa * w[D > 2 ? 1 : 0][b];
+            if (wab == 0.f) continue;
+            const int row = ((st[0] + a) * f.size[1] + (st[1] + b)) * f.size[2] + st[2];
+            const float vx = wab * v.x, vy = wab * v.y;
+#pragma unroll
+            for (int z = 0; z < K; ++z) {
+              const float wz = w[D - 1][z];
+              if (wz != 0.f) {
+                atomicAdd(re + row + z, wz * vx);
+                atomicAdd(im + row + z, wz * vy);
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+
+  // write-back, one warp per row of the tile
+  const int64_t gos = gp->gos;
+  const int64_t goff = (layout == kInternal ? gp->grid_off : gp->ugrid_off) + (int64_t)c0 * gos;
+  const int inner = f.size[D - 1];
+  const int outer = cells / inner;
+  const int nrows = ncg * outer;
+  const int nl = nos[D - 1];
+  const int s_first = wrap_once(f.org[D - 1] - hs[D - 1], nl);
+  for (int row = warp; row < nrows; row += kWarps) {
+    const int c = row / outer;
+    const int orow = row - c * outer;
+    int rr = orow;
+    int l[kMaxDim] = {0, 0, 0};
+#pragma unroll
+    for (int i = D - 2; i >= 0; --i) {
+      l[i] = rr % f.size[i];
+      rr /= f.size[i];
+    }
+    int64_t base = 0;
+#pragma unroll
+    for (int i = 0; i < D - 1; ++i) base = base * nos[i] + wrap_once(f.org[i] + l[i] - hs[i], nos[i]);
+    float2* dst = grid + goff + (int64_t)c * gos + base * nl;
+    const float* sre = acc_re + c * pstride + orow * inner;
+    const float* sim = acc_im + c * pstride + orow * inner;
+    for (int q = lane; q < inner; q += 32) {
+      int s = s_first + q;
+      if (s >= nl) s -= nl;
+      const float2 v = make_float2(sre[q], sim[q]);
+      if (it.split) {
+        atomicAdd(&dst[s].x, v.x);
+        atomicAdd(&dst[s].y, v.y);
+      } else {
+        dst[s] = v;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Launch helpers (called from tiles.cu when the fast path applies)
+// ---------------------------------------------------------------------------
+template <class Kern>
+static int prep_attr(Kern kernel, size_t smem) {
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e);
+  }
+  return MRN_OK;
+}
+
+#define MRN_FAST_G(G_, ...)                                        \
+  switch (G_) {                                                    \
+    case 1: { constexpr int GG = 1; __VA_ARGS__; } break;          \
+    case 2: case 4: { constexpr int GG = 4; __VA_ARGS__; } break;  \
+    case 8: { constexpr int GG = 8; __VA_ARGS__; } break;          \
+    case 16: { constexpr int GG = 16; __VA_ARGS__; } break;        \
+    default: { constexpr int GG = 32; __VA_ARGS__; } break;        \
+  }
+
+#define MRN_FAST_DK(D_, K_, ...)                                      \
+  do {                                                                \
+    if ((D_) == 2 && (K_) == 5) { constexpr int DD = 2, KK = 5; __VA_ARGS__; }       \
+    else if ((D_) == 2 && (K_) == 6) { constexpr int DD = 2, KK = 6; __VA_ARGS__; }  \
+    else if ((D_) == 2 && (K_) == 7) { constexpr int DD = 2, KK = 7; __VA_ARGS__; }  \
+    else if ((D_) == 2) { constexpr int DD = 2, KK = 8; __VA_ARGS__; }               \
+    else if ((K_) == 5) { constexpr int DD = 3, KK = 5; __VA_ARGS__; }               \
+    else if ((K_) == 6) { constexpr int DD = 3, KK = 6; __VA_ARGS__; }               \
+    else if ((K_) == 7) { constexpr int DD = 3, KK = 7; __VA_ARGS__; }               \
+    else { constexpr int DD = 3, KK = 8; __VA_ARGS__; }                              \
+  } while (0)
+
+bool fast_path_ok(const mrn_plan* P, bool gridding) {
+  if (P->ndim < 2) return false;
+  const int K = P->kb.ntaps[0];
+  if (K < 5 || K > 8) return false;
+  for (int i = 1; i < P->ndim; ++i)
+    if (P->kb.ntaps[i] != K) return false;
+  // region columns wrap at most once: every grid at least K cells wide
+  for (const auto& g : P->h_slices)
+    for (int i = 0; i < P->ndim; ++i)
+      if (g.nos[i] < K) return false;
+  if (gridding) {
+    for (const auto& g : P->h_slices)
+      for (int i = 0; i < P->ndim; ++i)
+        if (g.ntile[i] < 2) return false;
+  }
+  return true;
+}
+
+int launch_interp_fast(mrn_plan* P, const float2* grid, int layout, float2* ksp, float scale,
+                       const float2* temporal, int cg, int G, int pstride, size_t smem, dim3 gdim,
+                       cudaStream_t st) {
+  int rc = MRN_OK;
+  MRN_FAST_DK(P->ndim, P->kb.ntaps[0], MRN_FAST_G(G, {
+    auto kern = k_interp_fast<DD, KK, GG>;
+    rc = prep_attr(kern, smem);
+    if (rc == MRN_OK)
+      kern<<<gdim, kThreads, smem, st>>>(P->d_items_i, P->d_slices, P->kb, P->d_coord_i, P->d_perm_i,
+                                         grid, layout, ksp, scale, temporal, cg, pstride);
+  }));
+  if (rc != MRN_OK) return rc;
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? MRN_OK : cuda_fail(e);
+}
+
+int launch_grid_fast(mrn_plan* P, const float2* ksp, const float* dcf, const float2* temporal,
+                     int layout, float2* grid, float scale, int cg, int G, int pstride, size_t smem,
+                     dim3 gdim, cudaStream_t st) {
+  int rc = MRN_OK;
+  MRN_FAST_DK(P->ndim, P->kb.ntaps[0], MRN_FAST_G(G, {
+    auto kern = k_grid_fast<DD, KK, GG>;
+    rc = prep_attr(kern, smem);
+    if (rc == MRN_OK)
+      kern<<<gdim, kThreads, smem, st>>>(P->d_items_g, P->d_slices, P->kb, P->d_coord_g, P->d_perm_g,
+                                         ksp, dcf, temporal, grid, layout, scale, cg, pstride);
+  }));
+  if (rc != MRN_OK) return rc;
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? MRN_OK : cuda_fail(e);
+}
+
+}  // namespace mrn

@@ -151,8 +151,10 @@ class b200_nufft(NUFFT):
 
     def __init__(self, im_size: tuple, oversamp: Optional[float] = 1.25, width: Optional[int] = 6,
                  beta: Optional[float] = None, apodize: Optional[bool] = True,
-                 tile: Optional[tuple] = None, coil_group: int = 0, max_chunk: int = 0):
+                 tile: Optional[tuple] = None, coil_group: int = 0, max_chunk: int = 0,
+                 fast: bool = True):
         super().__init__(im_size)
+        self.fast = fast
         self.oversamp = oversamp
         self.width = width
         self.apodize = apodize
@@ -179,7 +181,7 @@ class b200_nufft(NUFFT):
         def make():
             p = Plan([tuple(self.im_size)] * N, [M] * N, [C] * N, self.oversamp, self._widths(),
                      self.beta, apodize=self.apodize, tile=self.tile, coil_group=self.coil_group,
-                     max_chunk=self.max_chunk, device=device)
+                     max_chunk=self.max_chunk, device=device, fast=self.fast)
             if trj is not None and M > 0:
                 p.set_traj(trj)
             return p

@@ -27,7 +27,7 @@ class Plan:
                  n_coil: Sequence[int], oversamp: float, width: Sequence[float],
                  beta: Optional[float] = None, raw: bool = False, apodize: bool = True,
                  tile: Optional[Sequence[int]] = None, coil_group: int = 0, max_chunk: int = 0,
-                 device: Optional[torch.device] = None):
+                 device: Optional[torch.device] = None, fast: bool = True):
         lib = _lib.load()
         self.lib = lib
         self.ndim = len(im_sizes[0])
@@ -53,6 +53,7 @@ class Plan:
             int(coil_group), int(max_chunk), self.device.index)
         check(rc, "mrn_plan_create")
         self.handle = h
+        check(lib.mrn_plan_set_option(h, _lib.MRN_OPT_FAST_KERNELS, 1 if fast else 0), "mrn_plan_set_option")
         n = self.nslices
         offs = [(C.c_int64 * n)() for _ in range(4)]
         check(lib.mrn_plan_offsets(h, *offs), "mrn_plan_offsets")

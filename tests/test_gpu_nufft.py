@@ -153,14 +153,15 @@ def _traj(kind, im, M, rng):
     raise ValueError(kind)
 
 
+@pytest.mark.parametrize("fast", [True, False], ids=["fast", "general"])
 @pytest.mark.parametrize("case", CASES, ids=lambda c: c[0])
-def test_oracle_parity_forward_adjoint_stages(case):
+def test_oracle_parity_forward_adjoint_stages(case, fast):
     name, im, os_, W, C, kind, M = case
     rng = np.random.RandomState(zlib.crc32(name.encode()) % (2 ** 31))
     trj = _traj(kind, im, M, rng)
     img = synth.randn_complex((1, C, *im), rng)
     ksp_in = synth.randn_complex((1, C, trj.shape[1]), rng)
-    nf = b200_nufft(im, oversamp=os_, width=W)
+    nf = b200_nufft(im, oversamp=os_, width=W, fast=fast)
     on = O.KBNufftOracle(im, os_, W)
     t = T(trj)
     assert rel(Nn(nf.forward(T(img), t)), on.forward(img, trj)) < TOL
@@ -364,9 +365,16 @@ def test_sense_cg_graph_matches_oracle():
     on = O.KBNufftOracle(im, 1.25, 6)
     Ao = O.SenseOracle(trj, mps, on)
     ksp = synth.add_noise(Ao.forward(truth), 30.0, rng)
-    ref = O.cg_sense(Ao, ksp, 8, 1e-3, 1.5)
+    # max eigenvalue of A^H A by the power method, x1.01 (recons.py:117-123)
+    v = synth.randn_complex(im, rng)
+    for _ in range(30):
+        z = Ao.normal(v)
+        lmax = float(np.linalg.norm(z))
+        v = (z / lmax).astype(np.complex64)
+    me = 1.01 * lmax
+    ref = O.cg_sense(Ao, ksp, 8, 1e-3, me)
     A = sense_linop(T(trj), T(mps), nufft=b200_nufft(im))
-    x_eager = CG_SENSE_recon(A, T(ksp), max_iter=8, lamda_l2=1e-3, max_eigen=1.5, verbose=False)
-    x_graph = CG_SENSE_recon(A, T(ksp), max_iter=8, lamda_l2=1e-3, max_eigen=1.5, verbose=False, graph=True)
+    x_eager = CG_SENSE_recon(A, T(ksp), max_iter=8, lamda_l2=1e-3, max_eigen=me, verbose=False)
+    x_graph = CG_SENSE_recon(A, T(ksp), max_iter=8, lamda_l2=1e-3, max_eigen=me, verbose=False, graph=True)
     assert rel(Nn(x_eager), ref) < 1e-4
     assert rel(Nn(x_graph), ref) < 1e-4
