@@ -56,7 +56,26 @@ struct KBParams {
   float radius[kMaxDim];  // W_i / 2
   float beta;
   int ntaps[kMaxDim];     // candidate taps floor(W_i) + 1
+  float inv_radius[kMaxDim];  // 1 / (W_i / 2)
 };
+
+// Tap weight from |dx| with a precomputed 1/r (the validity test |dx| <= r is
+// done by the caller in float32, exactly as the reference's mask); differs
+// from kb_tap only by the rounding of |dx|/r vs |dx|*(1/r) (<= 1 ulp).
+__device__ __forceinline__ float kb_tap_fast(float adx, float inv_r, float beta) {
+  const float x = adx * inv_r;
+  const float z = beta * sqrtf(fmaxf(1.0f - x * x, 0.0f));
+  if (z < 3.75f) {
+    const float y = (z * (1.0f / 3.75f)) * (z * (1.0f / 3.75f));
+    return 1.0f + y * (3.5156229f + y * (3.0899424f + y * (1.2067492f +
+                  y * (0.2659732f + y * (0.0360768f + y * 0.0045813f)))));
+  }
+  const float s = 3.75f * __frcp_rn(z);
+  const float p = 0.39894228f + s * (0.01328592f + s * (0.00225319f + s * (-0.00157565f +
+                  s * (0.00916281f + s * (-0.02057706f + s * (0.02635537f +
+                  s * (-0.01647633f + s * 0.00392377f)))))));
+  return expf(z) * rsqrtf(z) * p;
+}
 
 // --------------------------------------------------------------------------
 // Kaiser-Bessel kernel value I0(beta sqrt(1 - x^2)), x = |distance| / radius,
@@ -152,7 +171,8 @@ struct mrn_plan {
   double width[mrn::kMaxDim] = {1, 1, 1};
   double beta = 0.0;
   int tile[mrn::kMaxDim] = {1, 1, 1};
-  int coil_group = 1;
+  int coil_group = 1;      // coils per CTA chosen at plan creation (informational)
+  int coil_group_req = 0;  // caller's coil group, 0 = choose per kernel kind
   int max_coil = 1;
   int max_chunk = 1024;
   int tap_max = 8;  // compile-time tap bound used (8 or 16)

@@ -290,6 +290,7 @@ int mrn_plan_create(mrn_plan** out, int ndim, int n_slices, const int* im_size,
   for (int i = 0; i < ndim; ++i) {
     P->width[i] = width[i];
     P->kb.radius[i] = (float)width[i] / 2.0f;
+    P->kb.inv_radius[i] = 1.0f / P->kb.radius[i];
     P->kb.ntaps[i] = (int)std::floor(width[i]) + 1;
     maxtaps = std::max(maxtaps, P->kb.ntaps[i]);
   }
@@ -394,6 +395,7 @@ int mrn_plan_create(mrn_plan** out, int ndim, int n_slices, const int* im_size,
   if (pts >= (int64_t)INT32_MAX || maxe >= (int64_t)INT32_MAX) { delete P; return MRN_ERR_UNSUPPORTED; }
 
   // Coil group: all coils of the widest slice, limited by shared memory.
+  P->coil_group_req = coil_group > 0 ? std::min(coil_group, 64) : 0;
   if (coil_group > 0) {
     P->coil_group = std::min(coil_group, 64);
   } else {

@@ -676,7 +676,18 @@ static Layout plan_layout(const mrn_plan* P, int kind, bool fast = false) {
     cells *= (kind == 1) ? P->tmax_cells[i] : (P->tmax_cells[i] + P->kb.ntaps[i] - 1);
   const int pstride = (int)(cells | 1);
   const int KM = P->tap_max;
-  int cg = std::max(1, std::min(P->coil_group, P->max_coil));
+  int cg;
+  if (P->coil_group_req > 0) {
+    cg = std::max(1, std::min(P->coil_group_req, P->max_coil));
+  } else {
+    // about 76 KB of tile data per CTA (three CTAs per SM), at most 64 coils,
+    // coil groups balanced (same count, fewest coils per group)
+    const size_t target = 76 * 1024;
+    cg = (int)std::max<size_t>(1, target / ((size_t)pstride * 8));
+    cg = std::min(std::min(cg, 64), P->max_coil);
+    const int ng = (P->max_coil + cg - 1) / cg;
+    cg = (P->max_coil + ng - 1) / ng;
+  }
   Layout L{};
   for (;;) {
     const int G = pick_g(cg);

@@ -2,18 +2,20 @@
 // candidate taps per dimension K = floor(W) + 1 is a compile-time constant,
 // so the K^d tap loop is fully unrolled with immediate shared-memory offsets.
 //
-// Same algorithm and numerics as tiles.cu (tap j = lo + q, lo = ceil(u - W/2),
-// valid iff |(float)j - u| <= W/2, separable KB weights, circular cells);
-// the differences are in the instruction stream only:
+// Same algorithm and tap selection as tiles.cu (tap j = lo + q,
+// lo = ceil(u - W/2), valid iff |(float)j - u| <= W/2 in float32, separable
+// KB weights, circular cells); the differences are in the instruction stream:
 //   * the d*K 1D weights of a sample are computed once by the G lanes that
-//     share it (one weight per lane) and broadcast with warp shuffles;
+//     share it (one weight per lane, with 1/r precomputed) and broadcast with
+//     warp shuffles;
 //   * an invalid tap (outside the kernel support, or, for gridding, outside
-//     the tile this CTA owns) gets weight 0 and is skipped by a predicate,
-//     so there is no data-dependent loop bound;
+//     the tile this CTA owns) gets weight 0 in the lane that produces it and
+//     is skipped by a predicate, so there is no data-dependent loop bound;
+//   * the next sample's coordinates and index are loaded one iteration ahead;
 //   * no integer division in the per-sample path.
-// Used when every dimension has the same K in {5,6,7,8} (W in [4, 8)) and
-// d in {2, 3}; gridding additionally needs >= 2 tiles per dimension (so a
-// footprint meets a tile in one contiguous run).
+// Used when every dimension has the same K in {5,6,7,8} (W in [4, 8)), d is
+// 2 or 3 and every grid is at least K cells wide; gridding additionally needs
+// >= 2 tiles per dimension (so a footprint meets a tile in one contiguous run).
 #include <algorithm>
 
 #include "common.cuh"
@@ -55,14 +57,17 @@ __device__ __forceinline__ int wrap_once(int a, int n) {
   return a >= n ? a - n : a;
 }
 
-__device__ __forceinline__ float sel3(const float* v, int i) { return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]); }
-__device__ __forceinline__ int sel3i(const int* v, int i) { return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]); }
+template <class T>
+__device__ __forceinline__ T sel3(const T* v, int i) { return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]); }
 
 // 1D weights of one sample, w[i][q] for dim i, tap q (0 when invalid). The G
-// lanes of a slot compute D*K entries round-robin and exchange them by shuffles.
-template <int D, int K, int G>
-__device__ __forceinline__ void sample_weights(const float* u, const int* lo, const float* r,
-                                               float beta, int lane, float (&w)[D][K]) {
+// lanes of a slot compute the D*K entries round-robin and exchange them by
+// shuffles. With OWN, taps whose local cell st[i] + q lies outside [0,
+// size[i]) are zeroed too (gridding into an owned tile).
+template <int D, int K, int G, bool OWN>
+__device__ __forceinline__ void sample_weights(const float* u, const int* lo, const int* st,
+                                               const int* size, const KBParams& kb, int lane,
+                                               float (&w)[D][K]) {
   constexpr int NW = D * K;
   constexpr int IT = (NW + G - 1) / G;
   const int lg = lane % G;
@@ -74,9 +79,14 @@ __device__ __forceinline__ void sample_weights(const float* u, const int* lo, co
     if (t < NW) {
       const int i = t / K;
       const int q = t - i * K;
-      const float ui = sel3(u, i), ri = sel3(r, i);
-      const float adx = fabsf(__fsub_rn((float)(sel3i(lo, i) + q), ui));
-      if (adx <= ri) v = kb_tap(adx, ri, beta);
+      const float ui = sel3(u, i), ri = sel3(kb.radius, i);
+      const float adx = fabsf(__fsub_rn((float)(sel3(lo, i) + q), ui));
+      bool ok = adx <= ri;
+      if (OWN) {
+        const int l = sel3(st, i) + q;
+        ok = ok && l >= 0 && l < sel3(size, i);
+      }
+      if (ok) v = kb_tap_fast(adx, sel3(kb.inv_radius, i), kb.beta);
     }
     mine[it] = v;
   }
@@ -97,7 +107,7 @@ __device__ __forceinline__ void sample_weights(const float* u, const int* lo, co
   }
 }
 
-// Region loader (tile + halo, wrapped), one warp per row -- as tiles.cu.
+// Region loader (tile + halo, wrapped), one warp per row.
 template <int D>
 __device__ __forceinline__ void load_region_f(float2* __restrict__ tile, const float2* __restrict__ grid,
                                               int64_t goff, int64_t gos, const int* nos,
@@ -110,7 +120,6 @@ __device__ __forceinline__ void load_region_f(float2* __restrict__ tile, const f
   for (int i = 0; i < D - 1; ++i) outer *= ext[i];
   const int nrows = ncg * outer;
   const int nl = nos[D - 1];
-  // storage index of local column 0 and the local column where it wraps
   const int s_first = wrap_once(org[D - 1] - hs[D - 1], nl);
   for (int row = warp; row < nrows; row += kWarps) {
     const int c = row / outer;
@@ -148,6 +157,7 @@ k_interp_fast(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, 
               const float2* __restrict__ temporal, int cg, int pstride) {
   constexpr int SLOTS = 32 / G;
   constexpr int CPL = G == 32 ? 2 : 1;
+  constexpr int STRIDE = kWarps * SLOTS;
   extern __shared__ float4 smem_f4[];
   float2* tile = reinterpret_cast<float2*>(smem_f4);
 
@@ -169,28 +179,39 @@ k_interp_fast(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, 
   const int64_t gos = gp->gos;
   const int64_t goff = (layout == kInternal ? gp->grid_off : gp->ugrid_off) + (int64_t)c0 * gos;
   const int64_t m = gp->m, pt_off = gp->pt_off, ksp_off = gp->ksp_off;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int slot = lane / G, lg = lane % G;
+  // first sample of this warp, loaded before the region so the latencies overlap
+  int el = warp * SLOTS + slot;
+  const int ecl = it.count > 0 ? it.count - 1 : 0;  // interp items are never empty
+  float4 c_next = coord[it.start + min(el, ecl)];
+  int p_next = perm[it.start + min(el, ecl)];
+
   load_region_f<D>(tile, grid, goff, gos, nos, f.org, ext, hs, ncg, pstride);
   __syncthreads();
 
-  const float r[3] = {kb.radius[0], kb.radius[1], kb.radius[2]};
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int slot = lane / G, lg = lane % G;
-  for (int base = warp * SLOTS; base < it.count; base += kWarps * SLOTS) {
-    const int el = base + slot;
+  for (int base = warp * SLOTS; base < it.count; base += STRIDE) {
+    el = base + slot;
     const bool active = el < it.count;
-    const int e = it.start + (active ? el : 0);
-    const float4 c4 = coord[e];
+    const float4 c4 = c_next;
+    const int pm = p_next;
+    {
+      const int en = min(el + STRIDE, ecl);
+      c_next = coord[it.start + en];
+      p_next = perm[it.start + en];
+    }
     const float u[3] = {c4.x, c4.y, c4.z};
     int lo[3] = {0, 0, 0}, l0[3] = {0, 0, 0};
 #pragma unroll
     for (int i = 0; i < D; ++i) {
-      lo[i] = (int)ceilf(__fsub_rn(u[i], r[i]));
+      lo[i] = (int)ceilf(__fsub_rn(u[i], kb.radius[i]));
       l0[i] = wrap_once(lo[i], nos[i]) - f.org[i];
     }
     float w[D][K];
-    sample_weights<D, K, G>(u, lo, r, kb.beta, lane, w);
+    sample_weights<D, K, G, false>(u, lo, l0, f.size, kb, lane, w);
     if (!active) continue;
-    const int64_t lp = perm[e] - pt_off;
+    const int64_t lp = pm - pt_off;
     float2 h = make_float2(scale, 0.f);
     if (temporal) {
       const float2 t = temporal[pt_off + lp];
@@ -257,6 +278,7 @@ k_grid_fast(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
             int cg, int pstride) {
   constexpr int SLOTS = 32 / G;
   constexpr int CPL = G == 32 ? 2 : 1;
+  constexpr int STRIDE = kWarps * SLOTS;
   extern __shared__ float4 smem_f4[];
   float* acc_re = reinterpret_cast<float*>(smem_f4);
   float* acc_im = acc_re + (size_t)cg * pstride;
@@ -277,6 +299,16 @@ k_grid_fast(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
   int cells = 1;
 #pragma unroll
   for (int i = 0; i < D; ++i) cells *= f.size[i];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int slot = lane / G, lg = lane % G;
+  int el = warp * SLOTS + slot;
+  const int ecl = it.count > 0 ? it.count - 1 : 0;
+  float4 c_next = make_float4(0.f, 0.f, 0.f, 0.f);
+  int p_next = 0;
+  if (it.count > 0) {
+    c_next = coord[it.start + min(el, ecl)];
+    p_next = perm[it.start + min(el, ecl)];
+  }
   for (int idx = threadIdx.x; idx < ncg * pstride; idx += kThreads) {
     acc_re[idx] = 0.f;
     acc_im[idx] = 0.f;
@@ -284,35 +316,29 @@ k_grid_fast(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
   __syncthreads();
 
   const int64_t m = gp->m, pt_off = gp->pt_off, ksp_off = gp->ksp_off;
-  const float r[3] = {kb.radius[0], kb.radius[1], kb.radius[2]};
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int slot = lane / G, lg = lane % G;
-  for (int base = warp * SLOTS; base < it.count; base += kWarps * SLOTS) {
-    const int el = base + slot;
+  for (int base = warp * SLOTS; base < it.count; base += STRIDE) {
+    el = base + slot;
     const bool active = el < it.count;
-    const int e = it.start + (active ? el : 0);
-    const float4 c4 = coord[e];
+    const float4 c4 = c_next;
+    const int pm = p_next;
+    {
+      const int en = min(el + STRIDE, ecl);
+      c_next = coord[it.start + en];
+      p_next = perm[it.start + en];
+    }
     const float u[3] = {c4.x, c4.y, c4.z};
     int lo[3] = {0, 0, 0}, st[3] = {0, 0, 0};
 #pragma unroll
     for (int i = 0; i < D; ++i) {
-      lo[i] = (int)ceilf(__fsub_rn(u[i], r[i]));
+      lo[i] = (int)ceilf(__fsub_rn(u[i], kb.radius[i]));
       int s = wrap_once(lo[i], nos[i]) - f.org[i];
       if (s >= f.size[i]) s -= nos[i];  // footprint wraps into this tile from the end
       st[i] = s;
     }
     float w[D][K];
-    sample_weights<D, K, G>(u, lo, r, kb.beta, lane, w);
-    // taps outside the owned tile get weight 0
-#pragma unroll
-    for (int i = 0; i < D; ++i)
-#pragma unroll
-      for (int q = 0; q < K; ++q) {
-        const int l = st[i] + q;
-        if (l < 0 || l >= f.size[i]) w[i][q] = 0.f;
-      }
+    sample_weights<D, K, G, true>(u, lo, st, f.size, kb, lane, w);
     if (!active) continue;
-    const int64_t lp = perm[e] - pt_off;
+    const int64_t lp = pm - pt_off;
     float vs = scale;
     if (dcf) vs *= dcf[pt_off + lp];
     float2 h = make_float2(vs, 0.f);
@@ -442,7 +468,7 @@ static int prep_attr(Kern kernel, size_t smem) {
   } while (0)
 
 bool fast_path_ok(const mrn_plan* P, bool gridding) {
-  if (P->ndim < 2) return false;
+  if (!P->use_fast || P->ndim < 2) return false;
   const int K = P->kb.ntaps[0];
   if (K < 5 || K > 8) return false;
   for (int i = 1; i < P->ndim; ++i)
