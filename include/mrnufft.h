@@ -37,6 +37,7 @@ extern "C" {
 #define MRN_ERR_NOMEM (-5)    /* device allocation failed */
 #define MRN_ERR_STATE (-6)    /* plan used before mrn_plan_set_traj */
 #define MRN_ERR_UNSUPPORTED (-7)
+#define MRN_ERR_SCRATCH (-8)  /* problem larger than the fixed scratch of mrn_interp_noalloc */
 
 /* Plan flags */
 #define MRN_PLAN_RAW 1        /* im_size is the grid size itself; trajectories are grid
@@ -182,6 +183,29 @@ int mrn_cg_step(mrn_plan* plan, void* x, void* r, const void* p, const void* Ap,
 int mrn_cg_dir(mrn_plan* plan, const void* r, void* p, double* state, void* stream);
 /* Per-slice Re<a, b> in float64, accumulated into out[slice] (caller zeroes). */
 int mrn_cg_dot(mrn_plan* plan, const void* a, const void* b, double* out, void* stream);
+
+/*
+ * Type-2 interpolation that allocates nothing (no counterpart in the
+ * reference). For callers that cannot call cudaMalloc when they interpolate:
+ * work issued while a CUDA graph is being captured (allocation is not allowed
+ * there), real-time loops whose device memory is reserved up front, or hosts
+ * whose framework allocator owns all device memory. It needs no plan; its
+ * scratch is one fixed 32 MiB array in device memory that every GPU loading
+ * libmrnufft.so holds until the process exits.
+ * Result: the same as mrn_interp on an MRN_PLAN_RAW plan of this grid with
+ * scale 1 (ungrid, triton_interp/ungrid.py:34, kernel='kaiser_bessel',
+ * norm='1', pad_mode='circular'): grid [n_coil][grid_size...] complex64,
+ * locs [n_pts][ndim] float32 grid coordinates (wrapped), out [n_coil][n_pts].
+ * Limit: n_pts * ndim * (1 + K) * 4 bytes (+ 256) <= 32 MiB, K = floor(max
+ * width) + 1 -- about 524,000 samples for 2D width 6; larger calls return
+ * MRN_ERR_SCRATCH without launching anything. Calls share the scratch: calls
+ * that overlap on the GPU race and must be serialised by the caller. The
+ * first call on each device looks up the scratch's device address (with
+ * that device current); make that first call before any stream capture.
+ */
+int mrn_interp_noalloc(int ndim, const int* grid_size, int n_coil, int64_t n_pts,
+                       const double* width, double beta, const void* grid, const float* locs,
+                       void* out, void* stream);
 
 #ifdef __cplusplus
 }

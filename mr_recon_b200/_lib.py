@@ -23,6 +23,7 @@ MRN_ERR_CUFFT = -4
 MRN_ERR_NOMEM = -5
 MRN_ERR_STATE = -6
 MRN_ERR_UNSUPPORTED = -7
+MRN_ERR_SCRATCH = -8
 
 MRN_PLAN_RAW = 1
 MRN_PLAN_NO_APOD = 2
@@ -65,6 +66,7 @@ SIGNATURES = {
     "mrn_cg_step": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "mrn_cg_dir": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "mrn_cg_dot": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "mrn_interp_noalloc": (_i, [_i, _pi, _i, _i64, _pd, _d, _vp, _vp, _vp, _vp]),
 }
 
 _lib = None
@@ -104,7 +106,7 @@ def check(rc: int, what: str = "") -> None:
         msg += f" (cudaError {lib.mrn_last_cuda_error()})"
     if what:
         msg = f"{what}: {msg}"
-    if rc in (MRN_ERR_ARG, MRN_ERR_WIDTH):
+    if rc in (MRN_ERR_ARG, MRN_ERR_WIDTH, MRN_ERR_SCRATCH):
         raise ValueError(msg)
     if rc == MRN_ERR_UNSUPPORTED:
         raise NotImplementedError(msg)

@@ -258,6 +258,7 @@ const char* mrn_error_string(int code) {
     case MRN_ERR_NOMEM: return "device allocation failed";
     case MRN_ERR_STATE: return "trajectory not set on plan";
     case MRN_ERR_UNSUPPORTED: return "unsupported configuration";
+    case MRN_ERR_SCRATCH: return "problem exceeds the 32 MiB fixed scratch of mrn_interp_noalloc";
     default: return "unknown error";
   }
 }
