@@ -89,6 +89,15 @@ int mrn_plan_stats(mrn_plan* plan, int64_t* out4);
  * where they apply (2D/3D, equal width in [4, 8) per dimension); 0 forces the
  * general kernels. Both compute the same taps and weights. */
 #define MRN_OPT_FAST_KERNELS 1
+/* MRN_OPT_WARP_GRIDDING (default 1): 2D gridding with one warp per output tile
+ * (no atomics, reproducible summation order) where the fast kernels apply; 0
+ * uses the shared-memory-atomic tile kernel. */
+#define MRN_OPT_WARP_GRIDDING 2
+/* MRN_OPT_WEIGHT_TABLES (default 1): in 2D, mrn_plan_set_traj evaluates the KB
+ * weights of every sample once and stores them (~80 bytes per sample and per
+ * gridding entry); interpolation and gridding then read them instead of
+ * re-evaluating the kernel on every call. Set before mrn_plan_set_traj. */
+#define MRN_OPT_WEIGHT_TABLES 3
 int mrn_plan_set_option(mrn_plan* plan, int option, int value);
 
 /* Stage timing, a profiling aid with no counterpart in the reference (which

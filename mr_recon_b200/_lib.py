@@ -28,6 +28,8 @@ MRN_ERR_SCRATCH = -8
 MRN_PLAN_RAW = 1
 MRN_PLAN_NO_APOD = 2
 MRN_OPT_FAST_KERNELS = 1
+MRN_OPT_WARP_GRIDDING = 2
+MRN_OPT_WEIGHT_TABLES = 3
 
 _vp = C.c_void_p
 _i = C.c_int

@@ -20,9 +20,11 @@ constexpr int kWarps = kThreads / 32;
 struct SliceGeom {
   int n[kMaxDim];      // image size (1 for unused dims)
   int nos[kMaxDim];    // oversampled grid size (grid size for raw plans)
-  int ntile[kMaxDim];  // tiles per dim
+  int ntile[kMaxDim];  // interpolation tiles per dim
+  int gntile[kMaxDim]; // gridding tiles per dim
   int hshift[kMaxDim]; // Nos//2: centred index j lives at storage (j - hshift) mod Nos
-  int tile_base;       // first global tile id of this slice
+  int tile_base;       // first global interpolation tile id of this slice
+  int gtile_base;      // first global gridding tile id of this slice
   int ncoil;           // image batch (coils)
   int64_t m;           // samples
   int64_t pt_off;      // first global point id (offset into concatenated points)
@@ -170,22 +172,28 @@ struct mrn_plan {
   double oversamp = 1.0;
   double width[mrn::kMaxDim] = {1, 1, 1};
   double beta = 0.0;
-  int tile[mrn::kMaxDim] = {1, 1, 1};
+  int tile[mrn::kMaxDim] = {1, 1, 1};   // interpolation tile edge per dim
+  int gtile[mrn::kMaxDim] = {1, 1, 1};  // gridding tile edge per dim
+  bool warp_grid = true;  // 2D gridding with warp-private tiles (no atomics) where it applies
   int coil_group = 1;      // coils per CTA chosen at plan creation (informational)
   int coil_group_req = 0;  // caller's coil group, 0 = choose per kernel kind
   int max_coil = 1;
-  int max_chunk = 1024;
+  int max_chunk = 1024;   // samples per interpolation work item
+  int grid_chunk = 1024;  // entries per gridding work item
   int tap_max = 8;  // compile-time tap bound used (8 or 16)
   bool use_fast = true;  // use the unrolled fixed-K tile kernels where they apply
   mrn::KBParams kb{};
   std::vector<mrn::SliceGeom> h_slices;
   int64_t n_img = 0, n_ksp = 0, n_grid = 0, n_trj = 0, n_pts = 0, n_x = 0;
   int64_t n_prow = 0, n_irow = 0, n_xrow = 0;  // row counts of the grid / image layouts
-  int ntiles = 0;
-  int tmax_cells[mrn::kMaxDim] = {1, 1, 1};  // largest tile extent per dim over slices
+  int ntiles = 0;   // interpolation tiles, all slices
+  int ngtiles = 0;  // gridding tiles, all slices
+  int tmax_cells[mrn::kMaxDim] = {1, 1, 1};   // largest interpolation tile extent per dim
+  int tmax_gcells[mrn::kMaxDim] = {1, 1, 1};  // largest gridding tile extent per dim
   int64_t n_entries_grid = 0;  // gridding entries of the bound trajectory
   int64_t n_items_interp = 0, n_items_grid = 0, n_split = 0;
   int64_t cap_entries = 0, cap_items_i = 0, cap_items_g = 0;  // allocated capacities
+  int64_t cap_tiles = 0;
   bool traj_set = false;
 
   // device buffers
@@ -202,6 +210,17 @@ struct mrn_plan {
   int* d_val_a = nullptr;
   int* d_val_b = nullptr;
   float4* d_coord_tmp = nullptr;    // unsorted coords
+  // 2D weight tables (mrn_plan_set_traj; used when wtab_ok): per interpolation
+  // sample / gridding entry in sorted order, meta = {start0, start1, taps0,
+  // taps1} and the compacted valid (and, for gridding, in-tile) 1D weights,
+  // 8 per dimension, zero padded.
+  int4* d_wmeta_i = nullptr;
+  float4* d_wtab_i = nullptr;  // [entry][4] float4 = w0[0..7], w1[0..7]
+  int4* d_wmeta_g = nullptr;
+  float4* d_wtab_g = nullptr;
+  int64_t cap_wtab_i = 0, cap_wtab_g = 0;
+  bool use_wtab = false;  // option: build and use weight tables (off: slower when L2 is cold)
+  bool wtab_ok = false;   // tables of the bound trajectory are valid
   int* d_pt_slice = nullptr;        // point -> slice
   int* d_entry_cnt = nullptr;       // per point gridding entries (scan input/output)
   int* d_tile_start_i = nullptr;    // per global tile

@@ -26,6 +26,16 @@ bool fast_path_ok(const mrn_plan* P, bool gridding);
 int launch_interp_fast(mrn_plan* P, const float2* grid, int layout, float2* ksp, float scale,
                        const float2* temporal, int cg, int G, int pstride, size_t smem, dim3 gdim,
                        cudaStream_t st);
+int launch_grid_warp(mrn_plan* P, const float2* ksp, const float* dcf, const float2* temporal,
+                     int layout, float2* grid, float scale, cudaStream_t st);
+// 2D weight tables (wtab.cu)
+bool wtab_applicable(const mrn_plan* P);
+int build_wtabs(mrn_plan* P, cudaStream_t st);
+int launch_interp_tab(mrn_plan* P, const float2* grid, int layout, float2* ksp, float scale,
+                      const float2* temporal, int cg, int G, int pstride, size_t smem, dim3 gdim,
+                      cudaStream_t st);
+int launch_grid_warp_tab(mrn_plan* P, const float2* ksp, const float* dcf, const float2* temporal,
+                         int layout, float2* grid, float scale, cudaStream_t st);
 int launch_grid_fast(mrn_plan* P, const float2* ksp, const float* dcf, const float2* temporal,
                      int layout, float2* grid, float scale, int cg, int G, int pstride, size_t smem,
                      dim3 gdim, cudaStream_t st);

@@ -43,11 +43,11 @@ __device__ __forceinline__ int find_slice_by_point(const SliceGeom* sl, int ns, 
   return lo;
 }
 
-__device__ __forceinline__ int find_slice_by_tile(const SliceGeom* sl, int ns, int t) {
+__device__ __forceinline__ int find_slice_by_tile(const SliceGeom* sl, int ns, int t, int gridding) {
   int lo = 0, hi = ns - 1;
   while (lo < hi) {
     int mid = (lo + hi + 1) >> 1;
-    if (sl[mid].tile_base <= t) lo = mid; else hi = mid - 1;
+    if ((gridding ? sl[mid].gtile_base : sl[mid].tile_base) <= t) lo = mid; else hi = mid - 1;
   }
   return lo;
 }
@@ -94,7 +94,7 @@ __global__ void k_prep_points(const SliceGeom* __restrict__ sl, int ns, int ndim
     const int t0 = tile_of(pos_mod(lo, g.nos[i]), g.nos[i], g.ntile[i]);
     lin = lin * g.ntile[i] + t0;
     int tiles[kMaxTaps];
-    ntouch *= dim_tiles(v, kb.radius[i], kb.ntaps[i], g.nos[i], g.ntile[i], tiles);
+    ntouch *= dim_tiles(v, kb.radius[i], kb.ntaps[i], g.nos[i], g.gntile[i], tiles);
   }
   coord[p] = make_float4(u[0], u[1], u[2], 0.f);
   key_i[p] = (unsigned)(g.tile_base + lin);
@@ -116,15 +116,15 @@ __global__ void k_emit_entries(const SliceGeom* __restrict__ sl, int ns, int ndi
   int tiles[kMaxDim][kMaxTaps];
   int nt[kMaxDim] = {1, 1, 1};
   for (int i = 0; i < ndim; ++i)
-    nt[i] = dim_tiles(uu[i], kb.radius[i], kb.ntaps[i], g.nos[i], g.ntile[i], tiles[i]);
+    nt[i] = dim_tiles(uu[i], kb.radius[i], kb.ntaps[i], g.nos[i], g.gntile[i], tiles[i]);
   int o = eoff[p];
   for (int a = 0; a < nt[0]; ++a)
     for (int b = 0; b < (ndim > 1 ? nt[1] : 1); ++b)
       for (int c = 0; c < (ndim > 2 ? nt[2] : 1); ++c) {
         int lin = tiles[0][a];
-        if (ndim > 1) lin = lin * g.ntile[1] + tiles[1][b];
-        if (ndim > 2) lin = lin * g.ntile[2] + tiles[2][c];
-        key[o] = (unsigned)(g.tile_base + lin);
+        if (ndim > 1) lin = lin * g.gntile[1] + tiles[1][b];
+        if (ndim > 2) lin = lin * g.gntile[2] + tiles[2][c];
+        key[o] = (unsigned)(g.gtile_base + lin);
         val[o] = (int)p;
         ++o;
       }
@@ -158,16 +158,16 @@ __global__ void k_emit_items(const SliceGeom* __restrict__ sl, int ns, const int
                              const int* __restrict__ end, const int* __restrict__ nitems,
                              const int* __restrict__ ioff, int ntiles, int chunk,
                              Item* __restrict__ items, int* __restrict__ split_tiles,
-                             int* __restrict__ counts, int count_slot, int split_slot) {
+                             int* __restrict__ counts, int count_slot, int split_slot, int gridding) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ntiles) return;
   const int n = nitems[t];
-  const int s = find_slice_by_tile(sl, ns, t);
+  const int s = find_slice_by_tile(sl, ns, t, gridding);
   const int c = end[t] - start[t];
   for (int q = 0; q < n; ++q) {
     Item it;
     it.slice = s;
-    it.tile = t - sl[s].tile_base;
+    it.tile = t - (gridding ? sl[s].gtile_base : sl[s].tile_base);
     it.start = start[t] + q * chunk;
     it.count = max(0, min(chunk, c - q * chunk));
     it.split = n > 1 ? 1 : 0;
@@ -187,6 +187,61 @@ __global__ void k_total(const int* __restrict__ off, const int* __restrict__ cnt
 }
 
 static inline unsigned blocks_for(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+// Tiles per dimension for an edge length: at most ceil(nos / edge), and each
+// tile at least K-1 cells wide so a kernel footprint touches at most two tiles
+// per dimension (balanced partition, tile_begin / tile_of).
+static int tiles_for(int nos, int edge, int K) {
+  int nt = (nos + edge - 1) / edge;
+  if (K > 1) nt = std::min(nt, std::max(1, nos / (K - 1)));
+  return std::max(1, nt);
+}
+
+// Reorder work items by decreasing entry count (stable), on the host.
+static int sort_items_longest_first(Item* d_items, int64_t n, cudaStream_t st) {
+  if (n <= 1) return MRN_OK;
+  std::vector<Item> h((size_t)n);
+  cudaError_t e = cudaMemcpyAsync(h.data(), d_items, (size_t)n * sizeof(Item), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e);
+  std::stable_sort(h.begin(), h.end(), [](const Item& a, const Item& b) { return a.count > b.count; });
+  e = cudaMemcpyAsync(d_items, h.data(), (size_t)n * sizeof(Item), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  return e == cudaSuccess ? MRN_OK : cuda_fail(e);
+}
+
+// Tile arrays are allocated for the larger of the two tilings.
+static int64_t tile_capacity(const mrn_plan* P) { return std::max(P->ntiles, P->ngtiles); }
+
+// Interpolation and gridding tilings of every slice, and their global tile ids.
+void compute_tiling(mrn_plan* P) {
+  int tiles = 0, gtiles = 0;
+  for (int i = 0; i < kMaxDim; ++i) P->tmax_cells[i] = P->tmax_gcells[i] = 1;
+  for (auto& g : P->h_slices) {
+    int tc = 1, gc = 1;
+    for (int i = 0; i < kMaxDim; ++i) {
+      if (i >= P->ndim) {
+        g.ntile[i] = g.gntile[i] = 1;
+        continue;
+      }
+      const int K = P->kb.ntaps[i];
+      const int nt = tiles_for(g.nos[i], P->tile[i], K);
+      const int gt = tiles_for(g.nos[i], P->gtile[i], K);
+      g.ntile[i] = nt;
+      g.gntile[i] = gt;
+      tc *= nt;
+      gc *= gt;
+      P->tmax_cells[i] = std::max(P->tmax_cells[i], (g.nos[i] + nt - 1) / nt);
+      P->tmax_gcells[i] = std::max(P->tmax_gcells[i], (g.nos[i] + gt - 1) / gt);
+    }
+    g.tile_base = tiles;
+    g.gtile_base = gtiles;
+    tiles += tc;
+    gtiles += gc;
+  }
+  P->ntiles = tiles;
+  P->ngtiles = gtiles;
+}
 
 static cudaEvent_t pool_event(mrn_plan* P) {
   if (!P->ev_pool.empty()) {
@@ -317,12 +372,15 @@ int mrn_plan_create(mrn_plan** out, int ndim, int n_slices, const int* im_size,
   int deftile[kMaxDim];
   for (int i = 0; i < ndim; ++i) deftile[i] = (ndim == 1) ? 256 : (ndim == 2 ? 16 : 8);
   for (int i = 0; i < ndim; ++i) P->tile[i] = tile ? tile[i] : deftile[i];
+  // gridding tiles: 8x8 in 2D (one warp owns a tile), else the interpolation tile
+  for (int i = 0; i < ndim; ++i) P->gtile[i] = (ndim == 2 && !tile) ? 8 : P->tile[i];
   P->max_chunk = max_chunk > 0 ? max_chunk : 1024;
+  // one warp grids a 2D tile item alone: shorter items keep warps balanced
+  P->grid_chunk = max_chunk > 0 ? max_chunk : (ndim == 2 ? 256 : 1024);
 
   // Slices
   int64_t img = 0, ksp = 0, ugrid = 0, trjo = 0, pts = 0, xo = 0;
   int64_t prow = 0, irow = 0, xrow = 0;
-  int tiles = 0;
   int64_t maxe = 0;
   int64_t apodn = 0;
   P->h_slices.resize(n_slices);
@@ -333,7 +391,6 @@ int mrn_plan_create(mrn_plan** out, int ndim, int n_slices, const int* im_size,
     for (int i = 0; i < kMaxDim; ++i) {
       g.n[i] = 1; g.nos[i] = 1; g.ntile[i] = 1; g.hshift[i] = 0; g.scale[i] = 1.f; g.shift[i] = 0.f;
     }
-    int tcount = 1;
     for (int i = 0; i < ndim; ++i) {
       const int n = im_size[s * ndim + i];
       const int nos = raw ? n : (int)std::ceil(oversamp * n);
@@ -342,22 +399,12 @@ int mrn_plan_create(mrn_plan** out, int ndim, int n_slices, const int* im_size,
       g.hshift[i] = raw ? 0 : nos / 2;
       g.scale[i] = raw ? 1.0f : (float)((double)nos / (double)n);
       g.shift[i] = raw ? 0.0f : (float)(nos / 2);
-      const int K = P->kb.ntaps[i];
-      // tiles: at most ceil(nos / tile); each tile at least K-1 cells wide so a
-      // footprint touches at most two tiles per dimension
-      int nt = (nos + P->tile[i] - 1) / P->tile[i];
-      if (K > 1) nt = std::min(nt, std::max(1, nos / (K - 1)));
-      nt = std::max(1, nt);
-      g.ntile[i] = nt;
-      tcount *= nt;
       nimg *= n;
       gos *= nos;
-      spans *= (nt == 1 ? 1 : 2);
-      P->tmax_cells[i] = std::max(P->tmax_cells[i], (nos + nt - 1) / nt);
+      spans *= 2;
       g.apod_off[i] = (int)apodn;
       apodn += n;
     }
-    g.tile_base = tiles;
     g.ncoil = n_coil[s];
     g.m = n_pts[s];
     g.pt_off = pts;
@@ -374,7 +421,6 @@ int mrn_plan_create(mrn_plan** out, int ndim, int n_slices, const int* im_size,
     prow += (int64_t)g.ncoil * gos / g.nos[ndim - 1];
     irow += (int64_t)g.ncoil * nimg / g.n[ndim - 1];
     xrow += nimg / g.n[ndim - 1];
-    tiles += tcount;
     img += (int64_t)g.ncoil * nimg;
     ksp += (int64_t)g.ncoil * g.m;
     ugrid += (int64_t)g.ncoil * gos;
@@ -392,7 +438,7 @@ int mrn_plan_create(mrn_plan** out, int ndim, int n_slices, const int* im_size,
   P->n_prow = prow;
   P->n_irow = irow;
   P->n_xrow = xrow;
-  P->ntiles = tiles;
+  compute_tiling(P);
   if (pts >= (int64_t)INT32_MAX || maxe >= (int64_t)INT32_MAX) { delete P; return MRN_ERR_UNSUPPORTED; }
 
   // Coil group: all coils of the widest slice, limited by shared memory.
@@ -486,14 +532,19 @@ int mrn_plan_create(mrn_plan** out, int ndim, int n_slices, const int* im_size,
   PK(dev_alloc(&P->d_key_a, np));
   PK(dev_alloc(&P->d_val_a, np));
   PK(dev_alloc(&P->d_key_is, np));
-  PK(dev_alloc(&P->d_tile_start_i, tiles));
-  PK(dev_alloc(&P->d_tile_end_i, tiles));
-  PK(dev_alloc(&P->d_tile_start_g, tiles));
-  PK(dev_alloc(&P->d_tile_end_g, tiles));
-  PK(dev_alloc(&P->d_tile_nitems, tiles));
-  PK(dev_alloc(&P->d_tile_item_off, tiles));
+  {
+    // sized for the finest tiling either kind may get (plan options can change them)
+    const int64_t tmax = std::max<int64_t>(tile_capacity(P), 1);
+    PK(dev_alloc(&P->d_tile_start_i, tmax));
+    PK(dev_alloc(&P->d_tile_end_i, tmax));
+    PK(dev_alloc(&P->d_tile_start_g, tmax));
+    PK(dev_alloc(&P->d_tile_end_g, tmax));
+    PK(dev_alloc(&P->d_tile_nitems, tmax));
+    PK(dev_alloc(&P->d_tile_item_off, tmax));
+    PK(dev_alloc(&P->d_split_tiles, tmax));
+    P->cap_tiles = tmax;
+  }
   PK(dev_alloc(&P->d_counts, 8));
-  PK(dev_alloc(&P->d_split_tiles, tiles));
   PK(dev_alloc(&P->d_sync, 64));
   CK(cudaMemset(P->d_sync, 0, 64 * sizeof(unsigned)));
   if (!raw) {
@@ -516,6 +567,8 @@ int mrn_plan_set_option(mrn_plan* P, int option, int value) {
   if (!P) return MRN_ERR_ARG;
   switch (option) {
     case MRN_OPT_FAST_KERNELS: P->use_fast = value != 0; return MRN_OK;
+    case MRN_OPT_WARP_GRIDDING: P->warp_grid = value != 0; return MRN_OK;
+    case MRN_OPT_WEIGHT_TABLES: P->use_wtab = value != 0; return MRN_OK;
     default: return MRN_ERR_ARG;
   }
 }
@@ -555,7 +608,8 @@ int mrn_plan_destroy(mrn_plan* P) {
                   P->d_entry_cnt, P->d_tile_start_i, P->d_tile_end_i, P->d_tile_start_g,
                   P->d_tile_end_g, P->d_tile_nitems, P->d_tile_item_off, P->d_items_i,
                   P->d_items_g, P->d_counts, P->d_split_tiles, P->d_cub_tmp, P->d_grid,
-                  P->d_ksp_tmp, P->d_sync};
+                  P->d_ksp_tmp, P->d_sync, P->d_wmeta_i, P->d_wtab_i, P->d_wmeta_g,
+                  P->d_wtab_g};
   for (void* b : bufs)
     if (b) cudaFree(b);
   delete P;
@@ -592,10 +646,12 @@ int mrn_plan_set_traj(mrn_plan* P, const float* trj, void* stream_) {
   if (!P || (!trj && P->n_pts > 0)) return MRN_ERR_ARG;
   cudaStream_t st = (cudaStream_t)stream_;
   const int64_t M = P->n_pts;
-  const int T = P->ntiles;
+  const int T = P->ntiles;    // interpolation tiles
+  const int TG = P->ngtiles;  // gridding tiles
+  const int TT = std::max(T, TG);
   const int ndim = P->ndim;
   int bits = 1;
-  while (bits < 31 && (1ll << bits) <= (long long)T) ++bits;
+  while (bits < 31 && (1ll << bits) <= (long long)TT) ++bits;
   P->traj_set = false;
 
   // 1. coordinates, interpolation keys, gridding entry counts
@@ -604,7 +660,7 @@ int mrn_plan_set_traj(mrn_plan* P, const float* trj, void* stream_) {
   const int Mi = (int)std::max<int64_t>(M, 1);
   cub::DeviceScan::ExclusiveSum(nullptr, b, P->d_entry_cnt, eoff, Mi, st);
   need = std::max(need, b);
-  cub::DeviceScan::ExclusiveSum(nullptr, b, P->d_tile_nitems, P->d_tile_item_off, T, st);
+  cub::DeviceScan::ExclusiveSum(nullptr, b, P->d_tile_nitems, P->d_tile_item_off, TT, st);
   need = std::max(need, b);
   cub::DeviceRadixSort::SortPairs(nullptr, b, P->d_key_a, P->d_key_is, P->d_val_a, P->d_perm_i,
                                   Mi, 0, bits, st);
@@ -663,19 +719,20 @@ int mrn_plan_set_traj(mrn_plan* P, const float* trj, void* stream_) {
   // 4. per-tile ranges and work items
   CK(cudaMemsetAsync(P->d_tile_start_i, 0, T * sizeof(int), st));
   CK(cudaMemsetAsync(P->d_tile_end_i, 0, T * sizeof(int), st));
-  CK(cudaMemsetAsync(P->d_tile_start_g, 0, T * sizeof(int), st));
-  CK(cudaMemsetAsync(P->d_tile_end_g, 0, T * sizeof(int), st));
+  CK(cudaMemsetAsync(P->d_tile_start_g, 0, TG * sizeof(int), st));
+  CK(cudaMemsetAsync(P->d_tile_end_g, 0, TG * sizeof(int), st));
   CK(cudaMemsetAsync(P->d_counts, 0, 8 * sizeof(int), st));
   if (M > 0) {
     k_tile_ranges<<<blocks_for(M), 256, 0, st>>>(P->d_key_is, M, T, P->d_tile_start_i,
                                                  P->d_tile_end_i);
     if (E > 0)
-      k_tile_ranges<<<blocks_for(E), 256, 0, st>>>(P->d_key_g, E, T, P->d_tile_start_g,
+      k_tile_ranges<<<blocks_for(E), 256, 0, st>>>(P->d_key_g, E, TG, P->d_tile_start_g,
                                                    P->d_tile_end_g);
   }
   const int chunk = P->max_chunk;
+  const int gchunk = P->grid_chunk;
   const int64_t max_items_i = (int64_t)T + M / chunk + 1;
-  const int64_t max_items_g = (int64_t)T + E / chunk + 1;
+  const int64_t max_items_g = (int64_t)TG + E / gchunk + 1;
   if (P->cap_items_i < max_items_i) {
     RK(dev_alloc(&P->d_items_i, (size_t)max_items_i));
     P->cap_items_i = max_items_i;
@@ -690,22 +747,28 @@ int mrn_plan_set_traj(mrn_plan* P, const float* trj, void* stream_) {
   CK(cub::DeviceScan::ExclusiveSum(P->d_cub_tmp, b, P->d_tile_nitems, P->d_tile_item_off, T, st));
   k_emit_items<<<blocks_for(T), 256, 0, st>>>(P->d_slices, P->nslices, P->d_tile_start_i,
                                               P->d_tile_end_i, P->d_tile_nitems, P->d_tile_item_off,
-                                              T, chunk, P->d_items_i, nullptr, P->d_counts, 0, -1);
-  k_item_counts<<<blocks_for(T), 256, 0, st>>>(P->d_tile_start_g, P->d_tile_end_g, T, chunk, 1,
-                                               P->d_tile_nitems);
+                                              T, chunk, P->d_items_i, nullptr, P->d_counts, 0, -1,
+                                              0);
+  k_item_counts<<<blocks_for(TG), 256, 0, st>>>(P->d_tile_start_g, P->d_tile_end_g, TG, gchunk, 1,
+                                                P->d_tile_nitems);
   b = P->cub_tmp_bytes;
-  CK(cub::DeviceScan::ExclusiveSum(P->d_cub_tmp, b, P->d_tile_nitems, P->d_tile_item_off, T, st));
-  k_emit_items<<<blocks_for(T), 256, 0, st>>>(P->d_slices, P->nslices, P->d_tile_start_g,
-                                              P->d_tile_end_g, P->d_tile_nitems, P->d_tile_item_off,
-                                              T, chunk, P->d_items_g, P->d_split_tiles, P->d_counts,
-                                              1, 3);
+  CK(cub::DeviceScan::ExclusiveSum(P->d_cub_tmp, b, P->d_tile_nitems, P->d_tile_item_off, TG, st));
+  k_emit_items<<<blocks_for(TG), 256, 0, st>>>(P->d_slices, P->nslices, P->d_tile_start_g,
+                                               P->d_tile_end_g, P->d_tile_nitems, P->d_tile_item_off,
+                                               TG, gchunk, P->d_items_g, P->d_split_tiles, P->d_counts,
+                                               1, 3, 1);
   CK(cudaGetLastError());
+  RK(build_wtabs(P, st));
   int hc[4] = {0, 0, 0, 0};
   CK(cudaMemcpyAsync(hc, P->d_counts, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   P->n_items_interp = hc[0];
   P->n_items_grid = hc[1];
   P->n_split = hc[3];
+  // Longest items first: CTAs are dispatched in index order, so the last wave
+  // then consists of short items instead of a few long tiles.
+  RK(sort_items_longest_first(P->d_items_i, P->n_items_interp, st));
+  RK(sort_items_longest_first(P->d_items_g, P->n_items_grid, st));
   P->traj_set = true;
   return MRN_OK;
 }

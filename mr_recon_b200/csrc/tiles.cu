@@ -34,18 +34,20 @@ struct TileFrame {
   int size[kMaxDim];  // tile cells per dim
 };
 
-__device__ __forceinline__ TileFrame tile_frame(const SliceGeom& g, int tile, int D) {
+__device__ __forceinline__ TileFrame tile_frame(const SliceGeom& g, int tile, int D,
+                                                bool gridding = false) {
   TileFrame f;
   int rem = tile;
   int tc[kMaxDim] = {0, 0, 0};
+  const int* nts = gridding ? g.gntile : g.ntile;
   for (int i = D - 1; i >= 0; --i) {
-    tc[i] = rem % g.ntile[i];
-    rem /= g.ntile[i];
+    tc[i] = rem % nts[i];
+    rem /= nts[i];
   }
   for (int i = 0; i < kMaxDim; ++i) {
     if (i < D) {
-      f.org[i] = tile_begin(tc[i], g.nos[i], g.ntile[i]);
-      f.size[i] = tile_begin(tc[i] + 1, g.nos[i], g.ntile[i]) - f.org[i];
+      f.org[i] = tile_begin(tc[i], g.nos[i], nts[i]);
+      f.size[i] = tile_begin(tc[i] + 1, g.nos[i], nts[i]) - f.org[i];
     } else {
       f.org[i] = 0;
       f.size[i] = 1;
@@ -285,7 +287,7 @@ k_grid(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBParam
   const int c0 = blockIdx.y * cg;
   if (c0 >= g.ncoil) return;
   const int ncg = min(cg, g.ncoil - c0);
-  const TileFrame f = tile_frame(g, it.tile, D);
+  const TileFrame f = tile_frame(g, it.tile, D, true);
   int cells = 1;
   for (int i = 0; i < D; ++i) cells *= f.size[i];
   for (int idx = threadIdx.x; idx < ncg * pstride; idx += kThreads) {
@@ -460,12 +462,12 @@ __global__ void k_zero_split(const int* __restrict__ split_tiles, const int* __r
     int lo = 0, hi = ns - 1;
     while (lo < hi) {
       int mid = (lo + hi + 1) >> 1;
-      if (sl[mid].tile_base <= t) lo = mid; else hi = mid - 1;
+      if (sl[mid].gtile_base <= t) lo = mid; else hi = mid - 1;
     }
     s = lo;
   }
   const SliceGeom& g = sl[s];
-  const TileFrame f = tile_frame(g, t - g.tile_base, D);
+  const TileFrame f = tile_frame(g, t - g.gtile_base, D, true);
   int hs[kMaxDim];
   for (int i = 0; i < kMaxDim; ++i) hs[i] = (i < D && layout == kInternal) ? g.hshift[i] : 0;
   int cells = 1;
@@ -673,7 +675,7 @@ static Layout plan_layout(const mrn_plan* P, int kind, bool fast = false) {
   const int D = P->ndim;
   int64_t cells = 1;
   for (int i = 0; i < D; ++i)
-    cells *= (kind == 1) ? P->tmax_cells[i] : (P->tmax_cells[i] + P->kb.ntaps[i] - 1);
+    cells *= (kind == 1) ? P->tmax_gcells[i] : (P->tmax_cells[i] + P->kb.ntaps[i] - 1);
   const int pstride = (int)(cells | 1);
   const int KM = P->tap_max;
   int cg;
@@ -744,6 +746,9 @@ int launch_interp(mrn_plan* P, const float2* grid, GridLayout layout, float2* ks
   const Layout L = plan_layout(P, 0, fast);
   const int G = pick_g(L.cg);
   dim3 gridDim((unsigned)P->n_items_interp, (unsigned)((P->max_coil + L.cg - 1) / L.cg));
+  if (fast && P->wtab_ok && P->use_wtab)
+    return launch_interp_tab(P, grid, (int)layout, ksp, scale, temporal, L.cg, G, L.pstride, L.smem,
+                             gridDim, st);
   if (fast)
     return launch_interp_fast(P, grid, (int)layout, ksp, scale, temporal, L.cg, G, L.pstride, L.smem,
                               gridDim, st);
@@ -782,6 +787,10 @@ int launch_grid_t(mrn_plan* P, const float2* ksp, const float* dcf, const float2
       k_zero_split<3><<<nb, 256, 0, st>>>(P->d_split_tiles, P->d_counts, P->d_slices, P->nslices, grid, (int)layout);
   }
   dim3 gridDim((unsigned)P->n_items_grid, (unsigned)((P->max_coil + L.cg - 1) / L.cg));
+  if (fast && P->ndim == 2 && P->warp_grid && P->wtab_ok && P->use_wtab)
+    return launch_grid_warp_tab(P, ksp, dcf, temporal, (int)layout, grid, scale, st);
+  if (fast && P->ndim == 2 && P->warp_grid)
+    return launch_grid_warp(P, ksp, dcf, temporal, (int)layout, grid, scale, st);
   if (fast)
     return launch_grid_fast(P, ksp, dcf, temporal, (int)layout, grid, scale, L.cg, G, L.pstride, L.smem,
                             gridDim, st);

@@ -30,19 +30,20 @@ struct Frame {
   int size[kMaxDim];
 };
 
-__device__ __forceinline__ Frame frame_of(const SliceGeom& g, int tile, int D) {
+__device__ __forceinline__ Frame frame_of(const SliceGeom& g, int tile, int D, bool gridding) {
   Frame f;
   int rem = tile;
   int tc[kMaxDim] = {0, 0, 0};
+  const int* nts = gridding ? g.gntile : g.ntile;
   for (int i = D - 1; i >= 0; --i) {
-    tc[i] = rem % g.ntile[i];
-    rem /= g.ntile[i];
+    tc[i] = rem % nts[i];
+    rem /= nts[i];
   }
 #pragma unroll
   for (int i = 0; i < kMaxDim; ++i) {
     if (i < D) {
-      f.org[i] = tile_begin(tc[i], g.nos[i], g.ntile[i]);
-      f.size[i] = tile_begin(tc[i] + 1, g.nos[i], g.ntile[i]) - f.org[i];
+      f.org[i] = tile_begin(tc[i], g.nos[i], nts[i]);
+      f.size[i] = tile_begin(tc[i] + 1, g.nos[i], nts[i]) - f.org[i];
     } else {
       f.org[i] = 0;
       f.size[i] = 1;
@@ -173,7 +174,7 @@ k_interp_fast(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, 
     nos[i] = gp->nos[i];
     hs[i] = (i < D && layout == kInternal) ? gp->hshift[i] : 0;
   }
-  const Frame f = frame_of(*gp, it.tile, D);
+  const Frame f = frame_of(*gp, it.tile, D, false);
 #pragma unroll
   for (int i = 0; i < kMaxDim; ++i) ext[i] = i < D ? f.size[i] + K - 1 : 1;
   const int64_t gos = gp->gos;
@@ -295,7 +296,7 @@ k_grid_fast(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
     nos[i] = gp->nos[i];
     hs[i] = (i < D && layout == kInternal) ? gp->hshift[i] : 0;
   }
-  const Frame f = frame_of(*gp, it.tile, D);
+  const Frame f = frame_of(*gp, it.tile, D, true);
   int cells = 1;
 #pragma unroll
   for (int i = 0; i < D; ++i) cells *= f.size[i];
@@ -435,6 +436,127 @@ k_grid_fast(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
 }
 
 // ---------------------------------------------------------------------------
+// 2D gridding with warp-private tiles. One warp per work item; lanes are
+// coils (CPL per lane); the warp alone owns its tile's accumulator, so each
+// tap is a plain float32 shared-memory read-modify-write (LDS.64, 2 FFMA,
+// STS.64) -- no atomics (shared-memory float atomics are compare-and-swap
+// loops on sm_100a) and a fixed summation order, so results are bitwise
+// reproducible (except tiles split over several items, which combine with
+// global atomics).
+// ---------------------------------------------------------------------------
+template <int K, int CPL>
+__global__ void __launch_bounds__(32)
+k_grid_warp(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBParams kb,
+            const float4* __restrict__ coord, const int* __restrict__ perm,
+            const float2* __restrict__ ksp, const float* __restrict__ dcf,
+            const float2* __restrict__ temporal, float2* __restrict__ grid, int layout, float scale,
+            int cg, int pstride) {
+  extern __shared__ float4 smem_f4[];
+  float2* acc = reinterpret_cast<float2*>(smem_f4);  // [cg][pstride]
+
+  const Item it = items[blockIdx.x];
+  const SliceGeom* gp = sl + it.slice;
+  const int ncoil = gp->ncoil;
+  const int c0 = blockIdx.y * cg;
+  if (c0 >= ncoil) return;
+  const int ncg = min(cg, ncoil - c0);
+  const int lane = threadIdx.x;
+  const int nos0 = gp->nos[0], nos1 = gp->nos[1];
+  const int hs0 = layout == kInternal ? gp->hshift[0] : 0;
+  const int hs1 = layout == kInternal ? gp->hshift[1] : 0;
+  const Frame f = frame_of(*gp, it.tile, 2, true);
+  const int size1 = f.size[1];
+  const int cells = f.size[0] * size1;
+  const int ecl = it.count > 0 ? it.count - 1 : 0;
+  float4 c_next = make_float4(0.f, 0.f, 0.f, 0.f);
+  int p_next = 0;
+  if (it.count > 0) {
+    c_next = coord[it.start];
+    p_next = perm[it.start];
+  }
+  for (int idx = lane; idx < ncg * pstride; idx += 32) acc[idx] = make_float2(0.f, 0.f);
+  __syncwarp();
+
+  const int64_t m = gp->m, pt_off = gp->pt_off, ksp_off = gp->ksp_off;
+  for (int e = 0; e < it.count; ++e) {
+    const float4 c4 = c_next;
+    const int pm = p_next;
+    {
+      const int en = min(e + 1, ecl);
+      c_next = coord[it.start + en];
+      p_next = perm[it.start + en];
+    }
+    const float u[3] = {c4.x, c4.y, 0.f};
+    int lo[3] = {0, 0, 0}, st[3] = {0, 0, 0};
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      lo[i] = (int)ceilf(__fsub_rn(u[i], kb.radius[i]));
+      const int n = i == 0 ? nos0 : nos1;
+      int s = wrap_once(lo[i], n) - f.org[i];
+      if (s >= f.size[i]) s -= n;  // footprint wraps into this tile from the end
+      st[i] = s;
+    }
+    float w[2][K];
+    sample_weights<2, K, 32, true>(u, lo, st, f.size, kb, lane, w);
+    const int64_t lp = pm - pt_off;
+    float vs = scale;
+    if (dcf) vs *= dcf[pt_off + lp];
+    float2 h = make_float2(vs, 0.f);
+    if (temporal) {
+      const float2 t = temporal[pt_off + lp];
+      h = make_float2(vs * t.x, -vs * t.y);
+    }
+#pragma unroll
+    for (int q = 0; q < CPL; ++q) {
+      const int c = lane + q * 32;
+      if (c >= ncg) break;
+      const float2 a0 = __ldg(ksp + ksp_off + (int64_t)(c0 + c) * m + lp);
+      const float2 v = make_float2(a0.x * h.x - a0.y * h.y, a0.x * h.y + a0.y * h.x);
+      float2* plane = acc + c * pstride;
+#pragma unroll
+      for (int a = 0; a < K; ++a) {
+        const float wa = w[0][a];
+        if (wa == 0.f) continue;
+        float2* row = plane + (st[0] + a) * size1 + st[1];
+        const float vx = wa * v.x, vy = wa * v.y;
+#pragma unroll
+        for (int b = 0; b < K; ++b) {
+          const float wb = w[1][b];
+          if (wb != 0.f) {
+            float2 o = row[b];
+            o.x = fmaf(wb, vx, o.x);
+            o.y = fmaf(wb, vy, o.y);
+            row[b] = o;
+          }
+        }
+      }
+    }
+  }
+  __syncwarp();
+
+  // write-back: lanes over the cells of one coil plane at a time
+  const int64_t gos = gp->gos;
+  const int64_t goff = (layout == kInternal ? gp->grid_off : gp->ugrid_off) + (int64_t)c0 * gos;
+  for (int c = 0; c < ncg; ++c) {
+    float2* dstc = grid + goff + (int64_t)c * gos;
+    const float2* src = acc + c * pstride;
+    for (int cell = lane; cell < cells; cell += 32) {
+      const int l0 = cell / size1, l1 = cell - l0 * size1;
+      const int s0 = wrap_once(f.org[0] + l0 - hs0, nos0);
+      const int s1 = wrap_once(f.org[1] + l1 - hs1, nos1);
+      float2* d = dstc + (int64_t)s0 * nos1 + s1;
+      const float2 v = src[cell];
+      if (it.split) {
+        atomicAdd(&d->x, v.x);
+        atomicAdd(&d->y, v.y);
+      } else {
+        *d = v;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Launch helpers (called from tiles.cu when the fast path applies)
 // ---------------------------------------------------------------------------
 template <class Kern>
@@ -480,7 +602,7 @@ bool fast_path_ok(const mrn_plan* P, bool gridding) {
   if (gridding) {
     for (const auto& g : P->h_slices)
       for (int i = 0; i < P->ndim; ++i)
-        if (g.ntile[i] < 2) return false;
+        if (g.gntile[i] < 2) return false;
   }
   return true;
 }
@@ -496,6 +618,38 @@ int launch_interp_fast(mrn_plan* P, const float2* grid, int layout, float2* ksp,
       kern<<<gdim, kThreads, smem, st>>>(P->d_items_i, P->d_slices, P->kb, P->d_coord_i, P->d_perm_i,
                                          grid, layout, ksp, scale, temporal, cg, pstride);
   }));
+  if (rc != MRN_OK) return rc;
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? MRN_OK : cuda_fail(e);
+}
+
+int launch_grid_warp(mrn_plan* P, const float2* ksp, const float* dcf, const float2* temporal,
+                     int layout, float2* grid, float scale, cudaStream_t st) {
+  if (P->n_items_grid == 0) return MRN_OK;
+  const int pstride = (P->tmax_gcells[0] * P->tmax_gcells[1]) | 1;
+  int cg = P->coil_group_req > 0 ? std::min(P->coil_group_req, P->max_coil) : P->max_coil;
+  cg = std::max(1, std::min(cg, 64));
+  const int ng = (P->max_coil + cg - 1) / cg;
+  cg = (P->max_coil + ng - 1) / ng;
+  const size_t smem = (size_t)cg * pstride * sizeof(float2);
+  if (smem > 227 * 1024) return MRN_ERR_UNSUPPORTED;
+  const dim3 gdim((unsigned)P->n_items_grid, (unsigned)ng);
+  int rc = MRN_OK;
+  const int K = P->kb.ntaps[0];
+#define MRN_WARP_LAUNCH(KK, CP)                                                                   \
+  do {                                                                                            \
+    auto kern = k_grid_warp<KK, CP>;                                                              \
+    rc = prep_attr(kern, smem);                                                                   \
+    if (rc == MRN_OK)                                                                             \
+      kern<<<gdim, 32, smem, st>>>(P->d_items_g, P->d_slices, P->kb, P->d_coord_g, P->d_perm_g,   \
+                                   ksp, dcf, temporal, grid, layout, scale, cg, pstride);         \
+  } while (0)
+  const bool two = cg > 32;
+  if (K == 5) { if (two) MRN_WARP_LAUNCH(5, 2); else MRN_WARP_LAUNCH(5, 1); }
+  else if (K == 6) { if (two) MRN_WARP_LAUNCH(6, 2); else MRN_WARP_LAUNCH(6, 1); }
+  else if (K == 7) { if (two) MRN_WARP_LAUNCH(7, 2); else MRN_WARP_LAUNCH(7, 1); }
+  else { if (two) MRN_WARP_LAUNCH(8, 2); else MRN_WARP_LAUNCH(8, 1); }
+#undef MRN_WARP_LAUNCH
   if (rc != MRN_OK) return rc;
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? MRN_OK : cuda_fail(e);

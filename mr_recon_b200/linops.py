@@ -107,7 +107,8 @@ class sense_linop(linop):
                 M *= int(s)
             self.plan = Plan([im_size], [M], [ncoils], nufft.oversamp, nufft._widths(), nufft.beta,
                              apodize=nufft.apodize, tile=nufft.tile, coil_group=nufft.coil_group,
-                             max_chunk=nufft.max_chunk, device=dev, fast=nufft.fast)
+                             max_chunk=nufft.max_chunk, device=dev, fast=nufft.fast,
+                             warp_grid=nufft.warp_grid, weight_tables=nufft.weight_tables)
             self.plan.set_traj(trj.contiguous())
 
         if use_toeplitz:

@@ -27,7 +27,8 @@ class Plan:
                  n_coil: Sequence[int], oversamp: float, width: Sequence[float],
                  beta: Optional[float] = None, raw: bool = False, apodize: bool = True,
                  tile: Optional[Sequence[int]] = None, coil_group: int = 0, max_chunk: int = 0,
-                 device: Optional[torch.device] = None, fast: bool = True):
+                 device: Optional[torch.device] = None, fast: bool = True, warp_grid: bool = True,
+                 weight_tables: bool = False):
         lib = _lib.load()
         self.lib = lib
         self.ndim = len(im_sizes[0])
@@ -54,6 +55,10 @@ class Plan:
         check(rc, "mrn_plan_create")
         self.handle = h
         check(lib.mrn_plan_set_option(h, _lib.MRN_OPT_FAST_KERNELS, 1 if fast else 0), "mrn_plan_set_option")
+        check(lib.mrn_plan_set_option(h, _lib.MRN_OPT_WARP_GRIDDING, 1 if warp_grid else 0),
+              "mrn_plan_set_option")
+        check(lib.mrn_plan_set_option(h, _lib.MRN_OPT_WEIGHT_TABLES, 1 if weight_tables else 0),
+              "mrn_plan_set_option")
         n = self.nslices
         offs = [(C.c_int64 * n)() for _ in range(4)]
         check(lib.mrn_plan_offsets(h, *offs), "mrn_plan_offsets")

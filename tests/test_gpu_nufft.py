@@ -153,15 +153,21 @@ def _traj(kind, im, M, rng):
     raise ValueError(kind)
 
 
-@pytest.mark.parametrize("fast", [True, False], ids=["fast", "general"])
+# kernel paths: (fast kernels, warp-private 2D gridding, 2D weight tables)
+PATHS = {"tables": (True, True, True), "fast_warpgrid": (True, True, False),
+         "fast_atomicgrid": (True, False, False), "general": (False, False, False)}
+
+
+@pytest.mark.parametrize("path", list(PATHS))
 @pytest.mark.parametrize("case", CASES, ids=lambda c: c[0])
-def test_oracle_parity_forward_adjoint_stages(case, fast):
+def test_oracle_parity_forward_adjoint_stages(case, path):
     name, im, os_, W, C, kind, M = case
+    fast, warp, tables = PATHS[path]
     rng = np.random.RandomState(zlib.crc32(name.encode()) % (2 ** 31))
     trj = _traj(kind, im, M, rng)
     img = synth.randn_complex((1, C, *im), rng)
     ksp_in = synth.randn_complex((1, C, trj.shape[1]), rng)
-    nf = b200_nufft(im, oversamp=os_, width=W, fast=fast)
+    nf = b200_nufft(im, oversamp=os_, width=W, fast=fast, warp_grid=warp, weight_tables=tables)
     on = O.KBNufftOracle(im, os_, W)
     t = T(trj)
     assert rel(Nn(nf.forward(T(img), t)), on.forward(img, trj)) < TOL
