@@ -93,11 +93,24 @@ int mrn_plan_stats(mrn_plan* plan, int64_t* out4);
  * (no atomics, reproducible summation order) where the fast kernels apply; 0
  * uses the shared-memory-atomic tile kernel. */
 #define MRN_OPT_WARP_GRIDDING 2
-/* MRN_OPT_WEIGHT_TABLES (default 1): in 2D, mrn_plan_set_traj evaluates the KB
+/* MRN_OPT_WEIGHT_TABLES (default 0): in 2D, mrn_plan_set_traj evaluates the KB
  * weights of every sample once and stores them (~80 bytes per sample and per
  * gridding entry); interpolation and gridding then read them instead of
  * re-evaluating the kernel on every call. Set before mrn_plan_set_traj. */
 #define MRN_OPT_WEIGHT_TABLES 3
+/* Work decomposition (each takes effect at the next mrn_plan_set_traj):
+ * MRN_OPT_INTERP_CHUNK / MRN_OPT_GRID_CHUNK: samples per interpolation work
+ * item and gridding entries per gridding work item (defaults: 512 / 256 in
+ * 2D, 1024 otherwise); MRN_OPT_INTERP_TILE / MRN_OPT_GRID_TILE: tile edge in
+ * grid cells, every dimension (defaults: 16 / 8 in 2D, 8 in 3D, 256 in 1D). */
+#define MRN_OPT_INTERP_CHUNK 4
+#define MRN_OPT_GRID_CHUNK 5
+#define MRN_OPT_INTERP_TILE 6
+#define MRN_OPT_GRID_TILE 7
+/* MRN_OPT_REG_GRIDDING (default 1): 2D gridding tiles of at most 8x8 cells
+ * keep their accumulator in registers (two warps per tile, lane = coil);
+ * 0 keeps it in shared memory. Both sum in the same fixed order. */
+#define MRN_OPT_REG_GRIDDING 8
 int mrn_plan_set_option(mrn_plan* plan, int option, int value);
 
 /* Stage timing, a profiling aid with no counterpart in the reference (which

@@ -30,6 +30,11 @@ MRN_PLAN_NO_APOD = 2
 MRN_OPT_FAST_KERNELS = 1
 MRN_OPT_WARP_GRIDDING = 2
 MRN_OPT_WEIGHT_TABLES = 3
+MRN_OPT_INTERP_CHUNK = 4
+MRN_OPT_GRID_CHUNK = 5
+MRN_OPT_INTERP_TILE = 6
+MRN_OPT_GRID_TILE = 7
+MRN_OPT_REG_GRIDDING = 8
 
 _vp = C.c_void_p
 _i = C.c_int

@@ -175,6 +175,7 @@ struct mrn_plan {
   int tile[mrn::kMaxDim] = {1, 1, 1};   // interpolation tile edge per dim
   int gtile[mrn::kMaxDim] = {1, 1, 1};  // gridding tile edge per dim
   bool warp_grid = true;  // 2D gridding with warp-private tiles (no atomics) where it applies
+  bool reg_grid = true;   // ... with the tile accumulator in registers (tiles <= 8x8)
   int coil_group = 1;      // coils per CTA chosen at plan creation (informational)
   int coil_group_req = 0;  // caller's coil group, 0 = choose per kernel kind
   int max_coil = 1;

@@ -276,6 +276,31 @@ static int dev_alloc(T** p, size_t n) {
   return MRN_OK;
 }
 
+// New tile edges: recompute both tilings, grow the per-tile arrays when the
+// finer tiling needs more entries, refresh the device slice table. The bound
+// trajectory's binning is stale afterwards (mrn_plan_set_traj again).
+static int retile(mrn_plan* P) {
+  P->traj_set = false;
+  P->wtab_ok = false;
+  compute_tiling(P);
+  const int64_t need = std::max<int64_t>(tile_capacity(P), 1);
+  int rc = MRN_OK;
+  if (need > P->cap_tiles) {
+    int** bufs[] = {&P->d_tile_start_i, &P->d_tile_end_i, &P->d_tile_start_g, &P->d_tile_end_g,
+                    &P->d_tile_nitems, &P->d_tile_item_off, &P->d_split_tiles};
+    for (int** b : bufs)
+      if ((rc = dev_alloc(b, (size_t)need)) != MRN_OK) {
+        P->cap_tiles = 0;
+        return rc;
+      }
+    P->cap_tiles = need;
+  }
+  cudaError_t e = cudaSetDevice(P->device);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(P->d_slices, P->h_slices.data(), P->nslices * sizeof(SliceGeom), cudaMemcpyHostToDevice);
+  return e == cudaSuccess ? MRN_OK : cuda_fail(e);
+}
+
 static int ensure_cub(mrn_plan* P, size_t bytes) {
   if (bytes <= P->cub_tmp_bytes && P->d_cub_tmp) return MRN_OK;
   if (P->d_cub_tmp) cudaFree(P->d_cub_tmp);
@@ -374,7 +399,7 @@ int mrn_plan_create(mrn_plan** out, int ndim, int n_slices, const int* im_size,
   for (int i = 0; i < ndim; ++i) P->tile[i] = tile ? tile[i] : deftile[i];
   // gridding tiles: 8x8 in 2D (one warp owns a tile), else the interpolation tile
   for (int i = 0; i < ndim; ++i) P->gtile[i] = (ndim == 2 && !tile) ? 8 : P->tile[i];
-  P->max_chunk = max_chunk > 0 ? max_chunk : 1024;
+  P->max_chunk = max_chunk > 0 ? max_chunk : (ndim == 2 ? 512 : 1024);
   // one warp grids a 2D tile item alone: shorter items keep warps balanced
   P->grid_chunk = max_chunk > 0 ? max_chunk : (ndim == 2 ? 256 : 1024);
 
@@ -569,6 +594,19 @@ int mrn_plan_set_option(mrn_plan* P, int option, int value) {
     case MRN_OPT_FAST_KERNELS: P->use_fast = value != 0; return MRN_OK;
     case MRN_OPT_WARP_GRIDDING: P->warp_grid = value != 0; return MRN_OK;
     case MRN_OPT_WEIGHT_TABLES: P->use_wtab = value != 0; return MRN_OK;
+    case MRN_OPT_REG_GRIDDING: P->reg_grid = value != 0; return MRN_OK;
+    case MRN_OPT_INTERP_CHUNK:
+    case MRN_OPT_GRID_CHUNK:
+      if (value < 1) return MRN_ERR_ARG;
+      (option == MRN_OPT_INTERP_CHUNK ? P->max_chunk : P->grid_chunk) = value;
+      P->traj_set = false;  // items are cut at mrn_plan_set_traj
+      P->wtab_ok = false;
+      return MRN_OK;
+    case MRN_OPT_INTERP_TILE:
+    case MRN_OPT_GRID_TILE:
+      if (value < 1) return MRN_ERR_ARG;
+      for (int i = 0; i < P->ndim; ++i) (option == MRN_OPT_INTERP_TILE ? P->tile : P->gtile)[i] = value;
+      return retile(P);
     default: return MRN_ERR_ARG;
   }
 }
@@ -649,6 +687,7 @@ int mrn_plan_set_traj(mrn_plan* P, const float* trj, void* stream_) {
   const int T = P->ntiles;    // interpolation tiles
   const int TG = P->ngtiles;  // gridding tiles
   const int TT = std::max(T, TG);
+  if (P->cap_tiles < TT) return MRN_ERR_STATE;  // a failed retile left the tile arrays short
   const int ndim = P->ndim;
   int bits = 1;
   while (bits < 31 && (1ll << bits) <= (long long)TT) ++bits;

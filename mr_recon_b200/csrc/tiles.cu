@@ -451,6 +451,8 @@ k_grid(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBParam
 }
 
 // Zero every coil plane of the split gridding tiles before their items run.
+constexpr int kZeroCoils = 8;
+
 template <int D>
 __global__ void k_zero_split(const int* __restrict__ split_tiles, const int* __restrict__ counts,
                              const SliceGeom* __restrict__ sl, int ns, float2* __restrict__ grid,
@@ -472,13 +474,16 @@ __global__ void k_zero_split(const int* __restrict__ split_tiles, const int* __r
   for (int i = 0; i < kMaxDim; ++i) hs[i] = (i < D && layout == kInternal) ? g.hshift[i] : 0;
   int cells = 1;
   for (int i = 0; i < D; ++i) cells *= f.size[i];
-  const int c = blockIdx.y;  // one CTA per (split tile, coil)
-  if (c >= g.ncoil) return;
-  const int64_t goff = (layout == kInternal ? g.grid_off : g.ugrid_off) + (int64_t)c * g.gos;
-  for (int cell = threadIdx.x; cell < cells; cell += blockDim.x) {
+  // one CTA per (split tile, group of kZeroCoils coils)
+  const int cbeg = blockIdx.y * kZeroCoils;
+  const int ncl = min(kZeroCoils, g.ncoil - cbeg);
+  if (ncl <= 0) return;
+  const int64_t goff = (layout == kInternal ? g.grid_off : g.ugrid_off) + (int64_t)cbeg * g.gos;
+  for (int idx = threadIdx.x; idx < ncl * cells; idx += blockDim.x) {
+    const int c = idx / cells, cell = idx - c * cells;
     int64_t lin;
     tile_storage<D>(g, f, hs, cell, &lin);
-    grid[goff + lin] = make_float2(0.f, 0.f);
+    grid[goff + (int64_t)c * g.gos + lin] = make_float2(0.f, 0.f);
   }
 }
 
@@ -778,7 +783,7 @@ int launch_grid_t(mrn_plan* P, const float2* ksp, const float* dcf, const float2
   const Layout L = plan_layout(P, 1, fast);
   const int G = pick_g(L.cg);
   if (P->n_split > 0) {
-    const dim3 nb((unsigned)P->n_split, (unsigned)P->max_coil);
+    const dim3 nb((unsigned)P->n_split, (unsigned)((P->max_coil + kZeroCoils - 1) / kZeroCoils));
     if (P->ndim == 1)
       k_zero_split<1><<<nb, 256, 0, st>>>(P->d_split_tiles, P->d_counts, P->d_slices, P->nslices, grid, (int)layout);
     else if (P->ndim == 2)
@@ -787,6 +792,8 @@ int launch_grid_t(mrn_plan* P, const float2* ksp, const float* dcf, const float2
       k_zero_split<3><<<nb, 256, 0, st>>>(P->d_split_tiles, P->d_counts, P->d_slices, P->nslices, grid, (int)layout);
   }
   dim3 gridDim((unsigned)P->n_items_grid, (unsigned)((P->max_coil + L.cg - 1) / L.cg));
+  if (fast && P->ndim == 2 && P->warp_grid && grid_reg_ok(P))
+    return launch_grid_reg(P, ksp, dcf, temporal, (int)layout, grid, scale, st);
   if (fast && P->ndim == 2 && P->warp_grid && P->wtab_ok && P->use_wtab)
     return launch_grid_warp_tab(P, ksp, dcf, temporal, (int)layout, grid, scale, st);
   if (fast && P->ndim == 2 && P->warp_grid)

@@ -557,6 +557,211 @@ k_grid_warp(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
 }
 
 // ---------------------------------------------------------------------------
+// 2D gridding with the tile accumulator in registers. One block of two warps
+// per work item; lane = coil, warp w owns rows 4w..4w+3 of the (at most) 8x8
+// tile, so each lane keeps 4x8 complex cells in registers and every update
+// is a register FMA with a compile-time index: no shared-memory
+// read-modify-write, no atomics, float32 accumulation in a fixed order
+// (reproducible results).
+//
+// Entries run in batches of kRegBatch through an asynchronous pipeline
+// (cp.async), one barrier per batch. In iteration b:
+//   * the sample values (one 8-byte copy per entry and coil), densities and
+//     temporal weights of batch b+1 are copied into shared memory;
+//   * the coordinates and sample indices of batch b+3 are copied into a
+//     three-slot ring;
+//   * the 1D weights of batch b+1 are computed, already aligned to the
+//     tile's cells (zero outside the kernel support and the tile): thread
+//     (entry, dimension, half) evaluates 4 cells and stores them at once;
+//   * batch b accumulates: per entry, each of the warp's tile rows with a
+//     non-zero weight takes 2 x 8 FMAs per lane.
+// With at most 16 coils per group a warp runs SUB = 32 / CW entry streams of
+// CW lanes (CW = coil group rounded up to a power of two); their partial
+// tiles are summed with shuffles before the write-back.
+// ---------------------------------------------------------------------------
+constexpr int kRegTile = 8;
+constexpr int kRegRows = kRegTile / 2;  // tile rows per warp
+constexpr int kRegBatch = 16;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <int K, int SUB>
+__global__ void __launch_bounds__(64, 8)
+k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBParams kb,
+           const float4* __restrict__ coord, const int* __restrict__ perm,
+           const float2* __restrict__ ksp, const float* __restrict__ dcf,
+           const float2* __restrict__ temporal, float2* __restrict__ grid, int layout, float scale,
+           int cg) {
+  constexpr int T = kRegTile, R = kRegRows, B = kRegBatch, CW = 32 / SUB;
+  __shared__ float4 s_c[3][B];      // coordinate ring
+  __shared__ int s_pm[3][B];        // sample index ring
+  __shared__ float4 s_w[2][B][4];   // per entry: row weights (cells 0-7), column weights (cells 0-7)
+  __shared__ float2 s_v[2][B][CW];  // per entry and coil: sample value
+  __shared__ float s_d[2][B];       // per entry: density weight
+  __shared__ float2 s_t[2][B];      // per entry: temporal weight
+
+  const Item it = items[blockIdx.x];
+  const SliceGeom* gp = sl + it.slice;
+  const int ncoil = gp->ncoil;
+  const int c0 = blockIdx.y * cg;
+  if (c0 >= ncoil) return;
+  const int ncg = min(cg, ncoil - c0);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int coil = lane % CW, sub = lane / CW;
+  const int sid = warp * SUB + sub;  // copy stream of this thread
+  const bool has_coil = coil < ncg;
+  const int nos0 = gp->nos[0], nos1 = gp->nos[1];
+  const Frame f = frame_of(*gp, it.tile, 2, true);
+  const int64_t m = gp->m, pt_off = gp->pt_off;
+  const float2* kspc = ksp + gp->ksp_off + (int64_t)(c0 + (has_coil ? coil : 0)) * m;
+  const int nbatch = (it.count + B - 1) / B;
+  auto batch_len = [&](int bi) { return bi < nbatch ? min(B, it.count - bi * B) : 0; };
+
+  // coordinates and sample indices of batch bi into ring slot bi % 3
+  auto copy_coords = [&](int bi) {
+    const int nb = batch_len(bi), r3 = bi % 3;
+    if (tid < nb) cp_async16(&s_c[r3][tid], coord + it.start + bi * B + tid);
+    else if (tid >= 32 && tid - 32 < nb) cp_async4(&s_pm[r3][tid - 32], perm + it.start + bi * B + tid - 32);
+  };
+  // values (per entry and coil), densities and temporal weights of batch bi
+  auto copy_values = [&](int bi) {
+    const int nb = batch_len(bi), b2 = bi & 1, r3 = bi % 3;
+    if (has_coil)
+      for (int j = sid; j < nb; j += 2 * SUB) cp_async8(&s_v[b2][j][coil], kspc + (s_pm[r3][j] - pt_off));
+    if (tid < nb) {
+      if (dcf) cp_async4(&s_d[b2][tid], dcf + s_pm[r3][tid]);
+      else s_d[b2][tid] = 1.f;
+    } else if (tid >= 32 && tid - 32 < nb) {
+      if (temporal) cp_async8(&s_t[b2][tid - 32], temporal + s_pm[r3][tid - 32]);
+      else s_t[b2][tid - 32] = make_float2(1.f, 0.f);
+    }
+  };
+  // tile-aligned 1D weights of batch bi: thread = (entry, dimension, half of the cells)
+  auto weights = [&](int bi) {
+    const int j = tid >> 2, i = (tid >> 1) & 1, h = tid & 1;
+    if (j >= batch_len(bi)) return;
+    const float4 c4 = s_c[bi % 3][j];
+    const float u = i ? c4.y : c4.x;
+    const float r = i ? kb.radius[1] : kb.radius[0];
+    const float ir = i ? kb.inv_radius[1] : kb.inv_radius[0];
+    const int n = i ? nos1 : nos0;
+    const int size = i ? f.size[1] : f.size[0];
+    const int lo = (int)ceilf(__fsub_rn(u, r));
+    int st = wrap_once(lo, n) - (i ? f.org[1] : f.org[0]);
+    if (st >= size) st -= n;  // footprint wraps into this tile from the end
+    float w[4];
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      const int cell = 4 * h + l;
+      const int q = cell - st;
+      const float adx = fabsf(__fsub_rn((float)(lo + q), u));
+      w[l] = (q >= 0 && q < K && cell < size && adx <= r) ? kb_tap_fast(adx, ir, kb.beta) : 0.f;
+    }
+    s_w[bi & 1][j][2 * i + h] = make_float4(w[0], w[1], w[2], w[3]);
+  };
+
+  float2 acc[R][T];
+#pragma unroll
+  for (int a = 0; a < R; ++a)
+#pragma unroll
+    for (int b = 0; b < T; ++b) acc[a][b] = make_float2(0.f, 0.f);
+
+  copy_coords(0);
+  copy_coords(1);
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  copy_values(0);
+  cp_async_commit();
+  copy_coords(2);
+  cp_async_commit();
+  weights(0);
+  for (int bi = 0; bi < nbatch; ++bi) {
+    cp_async_wait<1>();  // values of bi and coordinates of bi + 1 have landed (this thread's)
+    __syncthreads();     // ... everyone's; weights of bi visible; buffers of bi - 1 free
+    copy_values(bi + 1);
+    cp_async_commit();
+    copy_coords(bi + 3);
+    cp_async_commit();
+    weights(bi + 1);
+    const int b2 = bi & 1, nb = batch_len(bi);
+    for (int j = sub; j < nb; j += SUB) {
+      const float4 rw = s_w[b2][j][warp];
+      const float4 q0 = s_w[b2][j][2], q1 = s_w[b2][j][3];
+      const float wr[R] = {rw.x, rw.y, rw.z, rw.w};
+      const float wc[T] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+      const float hs = scale * s_d[b2][j];
+      const float2 t = s_t[b2][j];
+      const float2 hh = make_float2(hs * t.x, -hs * t.y);
+      const float2 a0 = s_v[b2][j][coil];
+      const float2 val = make_float2(a0.x * hh.x - a0.y * hh.y, a0.x * hh.y + a0.y * hh.x);
+#pragma unroll
+      for (int a = 0; a < R; ++a) {
+        if (SUB == 1 && wr[a] == 0.f) continue;  // uniform: one entry per warp
+        const float vx = wr[a] * val.x, vy = wr[a] * val.y;
+#pragma unroll
+        for (int b = 0; b < T; ++b) {
+          acc[a][b].x = fmaf(wc[b], vx, acc[a][b].x);
+          acc[a][b].y = fmaf(wc[b], vy, acc[a][b].y);
+        }
+      }
+    }
+  }
+  cp_async_wait<0>();
+
+  if (SUB > 1) {
+#pragma unroll
+    for (int a = 0; a < R; ++a)
+#pragma unroll
+      for (int b = 0; b < T; ++b)
+#pragma unroll
+        for (int o = CW; o < 32; o <<= 1) {
+          acc[a][b].x += __shfl_xor_sync(0xffffffffu, acc[a][b].x, o);
+          acc[a][b].y += __shfl_xor_sync(0xffffffffu, acc[a][b].y, o);
+        }
+  }
+  if (!has_coil || sub != 0) return;
+  const int hs0 = layout == kInternal ? gp->hshift[0] : 0;
+  const int hs1 = layout == kInternal ? gp->hshift[1] : 0;
+  const int64_t gos = gp->gos;
+  float2* dst = grid + (layout == kInternal ? gp->grid_off : gp->ugrid_off) + (int64_t)(c0 + coil) * gos;
+  const int s1 = wrap_once(f.org[1] - hs1, nos1);
+#pragma unroll
+  for (int a = 0; a < R; ++a) {
+    const int row = warp * R + a;
+    if (row >= f.size[0]) break;
+    const int64_t rowo = (int64_t)wrap_once(f.org[0] + row - hs0, nos0) * nos1;
+#pragma unroll
+    for (int b = 0; b < T; ++b) {
+      if (b >= f.size[1]) break;
+      int s = s1 + b;
+      if (s >= nos1) s -= nos1;
+      float2* d = dst + rowo + s;
+      if (it.split) {
+        atomicAdd(&d->x, acc[a][b].x);
+        atomicAdd(&d->y, acc[a][b].y);
+      } else {
+        *d = acc[a][b];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Launch helpers (called from tiles.cu when the fast path applies)
 // ---------------------------------------------------------------------------
 template <class Kern>
@@ -651,6 +856,38 @@ int launch_grid_warp(mrn_plan* P, const float2* ksp, const float* dcf, const flo
   else { if (two) MRN_WARP_LAUNCH(8, 2); else MRN_WARP_LAUNCH(8, 1); }
 #undef MRN_WARP_LAUNCH
   if (rc != MRN_OK) return rc;
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? MRN_OK : cuda_fail(e);
+}
+
+bool grid_reg_ok(const mrn_plan* P) {
+  return P->reg_grid && P->ndim == 2 && P->tmax_gcells[0] <= kRegTile && P->tmax_gcells[1] <= kRegTile;
+}
+
+int launch_grid_reg(mrn_plan* P, const float2* ksp, const float* dcf, const float2* temporal,
+                    int layout, float2* grid, float scale, cudaStream_t st) {
+  if (P->n_items_grid == 0) return MRN_OK;
+  int cg = P->coil_group_req > 0 ? std::min(P->coil_group_req, P->max_coil) : P->max_coil;
+  cg = std::max(1, std::min(cg, 32));
+  const int ng = (P->max_coil + cg - 1) / cg;
+  cg = (P->max_coil + ng - 1) / ng;
+  // entry streams per warp: 32 lanes / (coil group rounded up to 8, 16 or 32)
+  const int sub = cg <= 8 ? 4 : (cg <= 16 ? 2 : 1);
+  const dim3 gdim((unsigned)P->n_items_grid, (unsigned)ng);
+  const int K = P->kb.ntaps[0];
+#define MRN_REG_LAUNCH(KK, SS)                                                              \
+  k_grid_reg<KK, SS><<<gdim, 64, 0, st>>>(P->d_items_g, P->d_slices, P->kb, P->d_coord_g, \
+                                          P->d_perm_g, ksp, dcf, temporal, grid, layout, scale, cg)
+#define MRN_REG_SUB(KK)                     \
+  if (sub == 4) MRN_REG_LAUNCH(KK, 4);      \
+  else if (sub == 2) MRN_REG_LAUNCH(KK, 2); \
+  else MRN_REG_LAUNCH(KK, 1)
+  if (K == 5) { MRN_REG_SUB(5); }
+  else if (K == 6) { MRN_REG_SUB(6); }
+  else if (K == 7) { MRN_REG_SUB(7); }
+  else { MRN_REG_SUB(8); }
+#undef MRN_REG_SUB
+#undef MRN_REG_LAUNCH
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? MRN_OK : cuda_fail(e);
 }

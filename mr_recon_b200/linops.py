@@ -108,7 +108,8 @@ class sense_linop(linop):
             self.plan = Plan([im_size], [M], [ncoils], nufft.oversamp, nufft._widths(), nufft.beta,
                              apodize=nufft.apodize, tile=nufft.tile, coil_group=nufft.coil_group,
                              max_chunk=nufft.max_chunk, device=dev, fast=nufft.fast,
-                             warp_grid=nufft.warp_grid, weight_tables=nufft.weight_tables)
+                             warp_grid=nufft.warp_grid, weight_tables=nufft.weight_tables,
+                             reg_grid=nufft.reg_grid)
             self.plan.set_traj(trj.contiguous())
 
         if use_toeplitz:

@@ -28,7 +28,7 @@ class Plan:
                  beta: Optional[float] = None, raw: bool = False, apodize: bool = True,
                  tile: Optional[Sequence[int]] = None, coil_group: int = 0, max_chunk: int = 0,
                  device: Optional[torch.device] = None, fast: bool = True, warp_grid: bool = True,
-                 weight_tables: bool = False):
+                 weight_tables: bool = False, reg_grid: bool = True):
         lib = _lib.load()
         self.lib = lib
         self.ndim = len(im_sizes[0])
@@ -58,6 +58,8 @@ class Plan:
         check(lib.mrn_plan_set_option(h, _lib.MRN_OPT_WARP_GRIDDING, 1 if warp_grid else 0),
               "mrn_plan_set_option")
         check(lib.mrn_plan_set_option(h, _lib.MRN_OPT_WEIGHT_TABLES, 1 if weight_tables else 0),
+              "mrn_plan_set_option")
+        check(lib.mrn_plan_set_option(h, _lib.MRN_OPT_REG_GRIDDING, 1 if reg_grid else 0),
               "mrn_plan_set_option")
         n = self.nslices
         offs = [(C.c_int64 * n)() for _ in range(4)]
@@ -95,6 +97,14 @@ class Plan:
         o = (C.c_int64 * 4)()
         check(self.lib.mrn_plan_stats(self.handle, o))
         return {"interp_items": o[0], "grid_items": o[1], "grid_entries": o[2], "split_tiles": o[3]}
+
+    def set_option(self, option: int, value: int) -> None:
+        """mrn_plan_set_option. Chunk and tile options take effect at the next
+        set_traj (the trajectory is unbound until then)."""
+        check(self.lib.mrn_plan_set_option(self.handle, int(option), int(value)), "mrn_plan_set_option")
+        if option in (_lib.MRN_OPT_INTERP_CHUNK, _lib.MRN_OPT_GRID_CHUNK, _lib.MRN_OPT_INTERP_TILE,
+                      _lib.MRN_OPT_GRID_TILE):
+            self.traj_bound = False
 
     STAGES = ("pre", "fft", "interp", "grid", "post", "layout_copy", "traj_grad", "cg")
 

@@ -130,6 +130,8 @@ CASES = [
     ("2d_spiral_os125_w6", (96, 80), 1.25, 6, 5, "spiral", 6000),
     ("2d_random_os2_w4_c1", (64, 64), 2.0, 4, 1, "random", 5000),
     ("2d_radial_os2_w7_c3", (64, 48), 2.0, 7, 3, "radial", 4096),
+    ("2d_spiral_os2_w5_c12", (64, 64), 2.0, 5, 12, "spiral", 3000),
+    ("2d_radial_os125_w8_c40", (48, 56), 1.25, 8, 40, "radial", 2048),
     ("3d_random_os125_w4", (20, 18, 22), 1.25, 4, 3, "random", 3000),
     ("3d_koosh_os15_w5_c17", (16, 16, 16), 1.5, 5, 17, "koosh", 2048),
     ("1d_random_os2_w6", (100,), 2.0, 6, 2, "random", 300),
@@ -153,21 +155,24 @@ def _traj(kind, im, M, rng):
     raise ValueError(kind)
 
 
-# kernel paths: (fast kernels, warp-private 2D gridding, 2D weight tables)
-PATHS = {"tables": (True, True, True), "fast_warpgrid": (True, True, False),
-         "fast_atomicgrid": (True, False, False), "general": (False, False, False)}
+# kernel paths: (fast kernels, warp-private 2D gridding, 2D weight tables,
+# register tile accumulator)
+PATHS = {"default_regtile": (True, True, False, True), "warp_smem": (True, True, False, False),
+         "tables": (True, True, True, False), "fast_atomicgrid": (True, False, False, False),
+         "general": (False, False, False, False)}
 
 
 @pytest.mark.parametrize("path", list(PATHS))
 @pytest.mark.parametrize("case", CASES, ids=lambda c: c[0])
 def test_oracle_parity_forward_adjoint_stages(case, path):
     name, im, os_, W, C, kind, M = case
-    fast, warp, tables = PATHS[path]
+    fast, warp, tables, reg = PATHS[path]
     rng = np.random.RandomState(zlib.crc32(name.encode()) % (2 ** 31))
     trj = _traj(kind, im, M, rng)
     img = synth.randn_complex((1, C, *im), rng)
     ksp_in = synth.randn_complex((1, C, trj.shape[1]), rng)
-    nf = b200_nufft(im, oversamp=os_, width=W, fast=fast, warp_grid=warp, weight_tables=tables)
+    nf = b200_nufft(im, oversamp=os_, width=W, fast=fast, warp_grid=warp, weight_tables=tables,
+                    reg_grid=reg)
     on = O.KBNufftOracle(im, os_, W)
     t = T(trj)
     assert rel(Nn(nf.forward(T(img), t)), on.forward(img, trj)) < TOL
@@ -194,6 +199,36 @@ def test_split_heavy_tiles_match_oracle():
     assert rel(Nn(nf.adjoint(T(y), T(trj))), on.adjoint(y, trj)) < TOL
     plan = nf._plans.entries[-1][2]
     assert plan.stats()["split_tiles"] > 0
+
+
+@pytest.mark.parametrize("opts", [dict(itile=12, gtile=6, ichunk=100, gchunk=40),
+                                  dict(itile=32, gtile=5, ichunk=4096, gchunk=2000),
+                                  dict(itile=9, gtile=20, ichunk=300, gchunk=64)])
+def test_plan_decomposition_options_rebind(opts):
+    """Changing tile edges and work-item sizes on a live plan re-bins the
+    trajectory at the next set_traj; results stay at oracle parity (gtile 20
+    leaves the register-tile kernel for the shared-memory one)."""
+    from mr_recon_b200 import _lib
+    rng = np.random.RandomState(5)
+    im, C = (80, 64), 6
+    trj = synth.vd_spiral(8, 900, 32.0).reshape(-1, 2)
+    img = synth.randn_complex((C, *im), rng)
+    y = synth.randn_complex((C, trj.shape[0]), rng)
+    on = O.KBNufftOracle(im, 1.25, 6)
+    p = Plan([im], [trj.shape[0]], [C], 1.25, (6.0, 6.0), device=DEV)
+    tr = T(trj)
+    p.set_traj(tr)
+    for opt, key in ((_lib.MRN_OPT_INTERP_TILE, "itile"), (_lib.MRN_OPT_GRID_TILE, "gtile"),
+                     (_lib.MRN_OPT_INTERP_CHUNK, "ichunk"), (_lib.MRN_OPT_GRID_CHUNK, "gchunk")):
+        p.set_option(opt, opts[key])
+    assert not p.traj_bound
+    p.set_traj(tr)
+    ksp = torch.empty(C * trj.shape[0], dtype=torch.complex64, device=DEV)
+    out = torch.empty(C * im[0] * im[1], dtype=torch.complex64, device=DEV)
+    p.forward(T(img).reshape(-1), ksp)
+    p.adjoint(T(y).reshape(-1), out)
+    assert rel(Nn(ksp).reshape(1, C, -1), on.forward(img[None], trj[None])) < TOL
+    assert rel(Nn(out).reshape(1, C, *im), on.adjoint(y[None], trj[None])) < TOL
 
 
 @pytest.mark.parametrize("tile", [(8, 8), (16, 32), (64, 64), (5, 7)])
