@@ -42,10 +42,10 @@ NCOIL = 32
 NINTL, NSAMP = 48, 2048
 OS, W = 1.25, 6
 WORKLOAD = "2D multi-coil KB NUFFT fwd+adj: 256x256 c64, 32 coils, VD spiral 48x2048, os 1.25, W 6"
-# DRAM traffic per gridding launch from an ncu capture of this workload
-# (profiles/grid_kernel_spiral256_c32.md); None until captured.
-GRID_TRAFFIC_BYTES = None
-INTERP_TRAFFIC_BYTES = None
+# DRAM bytes (read + write) per launch of each tile kernel on this workload,
+# from one ncu capture (profiles/grid_interp_kernels_spiral256_c32.md).
+GRID_TRAFFIC_BYTES = 33_542_912 + 44_800
+INTERP_TRAFFIC_BYTES = 25_538_560 + 97_792
 
 
 def load_peaks():
