@@ -751,6 +751,8 @@ int launch_interp(mrn_plan* P, const float2* grid, GridLayout layout, float2* ks
   const Layout L = plan_layout(P, 0, fast);
   const int G = pick_g(L.cg);
   dim3 gridDim((unsigned)P->n_items_interp, (unsigned)((P->max_coil + L.cg - 1) / L.cg));
+  if (fast && interp_reg_ok(P))
+    return launch_interp_reg(P, grid, (int)layout, ksp, scale, temporal, st);
   if (fast && P->wtab_ok && P->use_wtab)
     return launch_interp_tab(P, grid, (int)layout, ksp, scale, temporal, L.cg, G, L.pstride, L.smem,
                              gridDim, st);

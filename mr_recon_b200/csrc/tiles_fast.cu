@@ -557,6 +557,128 @@ k_grid_warp(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
 }
 
 // ---------------------------------------------------------------------------
+// 2D interpolation, lane = coil. The CTA stages its tile region (tile + K-1
+// halo, wrapped) for up to 32 coils in shared memory as [cell][coil] with an
+// odd coil stride CS = CW + 1: the transposing load writes without bank
+// conflicts and a warp reading one cell for all its coils touches
+// consecutive words. Each warp then takes one sample at a time (SUB samples
+// when the coil group is at most 16 / 8 wide): the 2K 1D weights are
+// computed once by the sample's lanes and broadcast with shuffles, and each
+// lane sums its coil's K x K taps row by row with packed two-lane FMAs
+// (fma.rn.f32x2: real and imaginary part in one instruction), one shared
+// load per tap.
+// ---------------------------------------------------------------------------
+constexpr int kRegInterpWarps = 8;
+constexpr int kInterpStage = 256;  // samples whose coordinates are staged at once
+
+template <int K, int SUB>
+__global__ void __launch_bounds__(kRegInterpWarps * 32)
+k_interp_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBParams kb,
+             const float4* __restrict__ coord, const int* __restrict__ perm,
+             const float2* __restrict__ grid, int layout, float2* __restrict__ ksp, float scale,
+             const float2* __restrict__ temporal, int cg) {
+  constexpr int CW = 32 / SUB, CS = CW + 1, NW = kRegInterpWarps, NT = NW * 32;
+  extern __shared__ float4 smem_f4[];
+  float2* region = reinterpret_cast<float2*>(smem_f4);
+  __shared__ float2 s_u[kInterpStage];  // coordinates of the staged samples
+  __shared__ int s_p[kInterpStage];     // their sample indices within the slice
+
+  const Item it = items[blockIdx.x];
+  const SliceGeom* gp = sl + it.slice;
+  const int ncoil = gp->ncoil;
+  const int c0 = blockIdx.y * cg;
+  if (c0 >= ncoil) return;
+  const int ncg = min(cg, ncoil - c0);
+  const int nos0 = gp->nos[0], nos1 = gp->nos[1];
+  const int hs0 = layout == kInternal ? gp->hshift[0] : 0;
+  const int hs1 = layout == kInternal ? gp->hshift[1] : 0;
+  const Frame f = frame_of(*gp, it.tile, 2, false);
+  const int ext0 = f.size[0] + K - 1, ext1 = f.size[1] + K - 1;
+  const int64_t gos = gp->gos;
+  const float2* gbase = grid + (layout == kInternal ? gp->grid_off : gp->ugrid_off) + (int64_t)c0 * gos;
+  const int64_t m = gp->m, pt_off = gp->pt_off;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int coil = lane % CW, sub = lane / CW;
+  const bool has_coil = coil < ncg;
+  float2* kspc = ksp + gp->ksp_off + (int64_t)(c0 + (has_coil ? coil : 0)) * m;
+
+  for (int sb = 0; sb < it.count; sb += kInterpStage) {
+    const int ns = min(kInterpStage, it.count - sb);
+    if (sb > 0) __syncthreads();  // every warp is done with the previous stage
+    for (int j = tid; j < ns; j += NT) {
+      const float4 c4 = coord[it.start + sb + j];
+      s_u[j] = make_float2(c4.x, c4.y);
+      s_p[j] = (int)(perm[it.start + sb + j] - pt_off);
+    }
+    if (sb == 0) {
+      // region: thread = one cell (r, q), looping over the coil planes with
+      // the global address stepped by the plane stride; kLoadBatch loads in
+      // flight per thread. Consecutive threads read consecutive cells of a
+      // row and write shared words 2 * CS apart (CS odd: no bank conflict).
+      constexpr int kLoadBatch = 8;
+      for (int cell = tid; cell < ext0 * ext1; cell += NT) {
+        const int r = cell / ext1, q = cell - r * ext1;
+        int s = wrap_once(f.org[1] - hs1, nos1) + q;
+        while (s >= nos1) s -= nos1;
+        const float2* src = gbase + (int64_t)wrap_once(f.org[0] + r - hs0, nos0) * nos1 + s;
+        float2* dst = region + cell * CS;
+        for (int cb = 0; cb < ncg; cb += kLoadBatch) {
+          float2 v[kLoadBatch];
+#pragma unroll
+          for (int u = 0; u < kLoadBatch; ++u)
+            if (cb + u < ncg) v[u] = __ldg(src + (int64_t)(cb + u) * gos);
+#pragma unroll
+          for (int u = 0; u < kLoadBatch; ++u)
+            if (cb + u < ncg) dst[cb + u] = v[u];
+        }
+      }
+    }
+    __syncthreads();
+
+    for (int base = warp * SUB; base < ns; base += NW * SUB) {
+      const int el = base + sub;
+      const bool active = el < ns;
+      const float2 uu = s_u[active ? el : base];
+      const float u[3] = {uu.x, uu.y, 0.f};
+      int lo[3] = {0, 0, 0}, l0[3] = {0, 0, 0};
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        lo[i] = (int)ceilf(__fsub_rn(u[i], kb.radius[i]));
+        l0[i] = wrap_once(lo[i], i == 0 ? nos0 : nos1) - f.org[i];
+      }
+      float w[2][K];
+      sample_weights<2, K, CW, false>(u, lo, l0, f.size, kb, lane, w);
+      if (!active || !has_coil) continue;
+      const float2* rb = region + (l0[0] * ext1 + l0[1]) * CS + coil;
+      float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int a = 0; a < K; ++a) {
+        if (w[0][a] == 0.f) continue;
+        const float2* rp = rb + a * ext1 * CS;
+        float2 ra = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int b = 0; b < K; ++b) ra = __ffma2_rn(make_float2(w[1][b], w[1][b]), rp[b * CS], ra);
+        acc = __ffma2_rn(make_float2(w[0][a], w[0][a]), ra, acc);
+      }
+      const int lp = s_p[el];
+      float2 h = make_float2(scale, 0.f);
+      if (temporal) {
+        const float2 t = temporal[pt_off + lp];
+        h = make_float2(scale * t.x, scale * t.y);
+      }
+      const float2 v = make_float2(acc.x * h.x - acc.y * h.y, acc.x * h.y + acc.y * h.x);
+      float2* dst = kspc + lp;
+      if (temporal) {
+        const float2 o = *dst;
+        *dst = make_float2(o.x + v.x, o.y + v.y);
+      } else {
+        *dst = v;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // 2D gridding with the tile accumulator in registers. One block of two warps
 // per work item; lane = coil, warp w owns rows 4w..4w+3 of the (at most) 8x8
 // tile, so each lane keeps 4x8 complex cells in registers and every update
@@ -855,6 +977,60 @@ int launch_grid_warp(mrn_plan* P, const float2* ksp, const float* dcf, const flo
   else if (K == 7) { if (two) MRN_WARP_LAUNCH(7, 2); else MRN_WARP_LAUNCH(7, 1); }
   else { if (two) MRN_WARP_LAUNCH(8, 2); else MRN_WARP_LAUNCH(8, 1); }
 #undef MRN_WARP_LAUNCH
+  if (rc != MRN_OK) return rc;
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? MRN_OK : cuda_fail(e);
+}
+
+static int interp_reg_sub(const mrn_plan* P, int* cg_out, int* ng_out) {
+  int cg = P->coil_group_req > 0 ? std::min(P->coil_group_req, P->max_coil) : P->max_coil;
+  cg = std::max(1, std::min(cg, 32));
+  const int ng = (P->max_coil + cg - 1) / cg;
+  cg = (P->max_coil + ng - 1) / ng;
+  *cg_out = cg;
+  *ng_out = ng;
+  return cg <= 8 ? 4 : (cg <= 16 ? 2 : 1);
+}
+
+static size_t interp_reg_smem(const mrn_plan* P, int sub) {
+  const int K = P->kb.ntaps[0];
+  return (size_t)(P->tmax_cells[0] + K - 1) * (P->tmax_cells[1] + K - 1) * (32 / sub + 1) * sizeof(float2);
+}
+
+bool interp_reg_ok(const mrn_plan* P) {
+  if (!P->reg_interp || P->ndim != 2) return false;
+  int cg, ng;
+  const int sub = interp_reg_sub(P, &cg, &ng);
+  return interp_reg_smem(P, sub) + kInterpStage * (sizeof(float2) + sizeof(int)) <= 227 * 1024;
+}
+
+int launch_interp_reg(mrn_plan* P, const float2* grid, int layout, float2* ksp, float scale,
+                      const float2* temporal, cudaStream_t st) {
+  if (P->n_items_interp == 0) return MRN_OK;
+  int cg, ng;
+  const int sub = interp_reg_sub(P, &cg, &ng);
+  const size_t smem = interp_reg_smem(P, sub);
+  const dim3 gdim((unsigned)P->n_items_interp, (unsigned)ng);
+  const int K = P->kb.ntaps[0];
+  int rc = MRN_OK;
+#define MRN_IREG_LAUNCH(KK, SS)                                                                     \
+  do {                                                                                              \
+    auto kern = k_interp_reg<KK, SS>;                                                               \
+    rc = prep_attr(kern, smem);                                                                     \
+    if (rc == MRN_OK)                                                                               \
+      kern<<<gdim, kRegInterpWarps * 32, smem, st>>>(P->d_items_i, P->d_slices, P->kb, P->d_coord_i, \
+                                                     P->d_perm_i, grid, layout, ksp, scale, temporal, cg); \
+  } while (0)
+#define MRN_IREG_SUB(KK)                     \
+  if (sub == 4) MRN_IREG_LAUNCH(KK, 4);      \
+  else if (sub == 2) MRN_IREG_LAUNCH(KK, 2); \
+  else MRN_IREG_LAUNCH(KK, 1)
+  if (K == 5) { MRN_IREG_SUB(5); }
+  else if (K == 6) { MRN_IREG_SUB(6); }
+  else if (K == 7) { MRN_IREG_SUB(7); }
+  else { MRN_IREG_SUB(8); }
+#undef MRN_IREG_SUB
+#undef MRN_IREG_LAUNCH
   if (rc != MRN_OK) return rc;
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? MRN_OK : cuda_fail(e);

@@ -153,10 +153,11 @@ class b200_nufft(NUFFT):
                  beta: Optional[float] = None, apodize: Optional[bool] = True,
                  tile: Optional[tuple] = None, coil_group: int = 0, max_chunk: int = 0,
                  fast: bool = True, warp_grid: bool = True, weight_tables: bool = False,
-                 reg_grid: bool = True):
+                 reg_grid: bool = True, reg_interp: bool = True):
         super().__init__(im_size)
         self.fast = fast
         self.reg_grid = reg_grid
+        self.reg_interp = reg_interp
         self.warp_grid = warp_grid
         self.weight_tables = weight_tables
         self.oversamp = oversamp
@@ -187,7 +188,7 @@ class b200_nufft(NUFFT):
                      self.beta, apodize=self.apodize, tile=self.tile, coil_group=self.coil_group,
                      max_chunk=self.max_chunk, device=device, fast=self.fast,
                      warp_grid=self.warp_grid, weight_tables=self.weight_tables,
-                     reg_grid=self.reg_grid)
+                     reg_grid=self.reg_grid, reg_interp=self.reg_interp)
             if trj is not None and M > 0:
                 p.set_traj(trj)
             return p

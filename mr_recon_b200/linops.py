@@ -109,7 +109,7 @@ class sense_linop(linop):
                              apodize=nufft.apodize, tile=nufft.tile, coil_group=nufft.coil_group,
                              max_chunk=nufft.max_chunk, device=dev, fast=nufft.fast,
                              warp_grid=nufft.warp_grid, weight_tables=nufft.weight_tables,
-                             reg_grid=nufft.reg_grid)
+                             reg_grid=nufft.reg_grid, reg_interp=nufft.reg_interp)
             self.plan.set_traj(trj.contiguous())
 
         if use_toeplitz:

@@ -28,7 +28,8 @@ class Plan:
                  beta: Optional[float] = None, raw: bool = False, apodize: bool = True,
                  tile: Optional[Sequence[int]] = None, coil_group: int = 0, max_chunk: int = 0,
                  device: Optional[torch.device] = None, fast: bool = True, warp_grid: bool = True,
-                 weight_tables: bool = False, reg_grid: bool = True):
+                 weight_tables: bool = False, reg_grid: bool = True,
+                 reg_interp: bool = True):
         lib = _lib.load()
         self.lib = lib
         self.ndim = len(im_sizes[0])
@@ -60,6 +61,8 @@ class Plan:
         check(lib.mrn_plan_set_option(h, _lib.MRN_OPT_WEIGHT_TABLES, 1 if weight_tables else 0),
               "mrn_plan_set_option")
         check(lib.mrn_plan_set_option(h, _lib.MRN_OPT_REG_GRIDDING, 1 if reg_grid else 0),
+              "mrn_plan_set_option")
+        check(lib.mrn_plan_set_option(h, _lib.MRN_OPT_REG_INTERP, 1 if reg_interp else 0),
               "mrn_plan_set_option")
         n = self.nslices
         offs = [(C.c_int64 * n)() for _ in range(4)]

@@ -155,24 +155,24 @@ def _traj(kind, im, M, rng):
     raise ValueError(kind)
 
 
-# kernel paths: (fast kernels, warp-private 2D gridding, 2D weight tables,
-# register tile accumulator)
-PATHS = {"default_regtile": (True, True, False, True), "warp_smem": (True, True, False, False),
-         "tables": (True, True, True, False), "fast_atomicgrid": (True, False, False, False),
-         "general": (False, False, False, False)}
+# kernel paths (b200_nufft options; the default is lane-per-coil interpolation
+# and register-tile gridding in 2D)
+PATHS = {"default": {},
+         "warp_smem": dict(reg_grid=False, reg_interp=False),
+         "tables": dict(weight_tables=True, reg_grid=False, reg_interp=False),
+         "fast_atomicgrid": dict(warp_grid=False, reg_interp=False),
+         "general": dict(fast=False)}
 
 
 @pytest.mark.parametrize("path", list(PATHS))
 @pytest.mark.parametrize("case", CASES, ids=lambda c: c[0])
 def test_oracle_parity_forward_adjoint_stages(case, path):
     name, im, os_, W, C, kind, M = case
-    fast, warp, tables, reg = PATHS[path]
     rng = np.random.RandomState(zlib.crc32(name.encode()) % (2 ** 31))
     trj = _traj(kind, im, M, rng)
     img = synth.randn_complex((1, C, *im), rng)
     ksp_in = synth.randn_complex((1, C, trj.shape[1]), rng)
-    nf = b200_nufft(im, oversamp=os_, width=W, fast=fast, warp_grid=warp, weight_tables=tables,
-                    reg_grid=reg)
+    nf = b200_nufft(im, oversamp=os_, width=W, **PATHS[path])
     on = O.KBNufftOracle(im, os_, W)
     t = T(trj)
     assert rel(Nn(nf.forward(T(img), t)), on.forward(img, trj)) < TOL
