@@ -136,6 +136,167 @@ def cpu_baseline(trj, imgs, coils, repeats=1):
     return coils * M * repeats / t_total / 1e6, threads, t_total
 
 
+def _events(torch):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def bench_c3(dev, steps, peak):
+    """3D NUFFT with autograd: 192^3, 16 coils, kooshball 20,000 x 384,
+    os 1.25, W 4. fwd+adj Msample*coil/s with the gridding roofline (the
+    path's HBM-bound case), and one loss / backward step with image and
+    trajectory gradients."""
+    import torch
+    from mr_recon_b200.fourier import b200_nufft
+    from mr_recon_b200 import synth
+    N, C = 192, 16
+    trj = torch.from_numpy(synth.kooshball(20000, 384, N / 2.0).reshape(1, -1, 3)).to(dev)
+    M = trj.shape[1]
+    g = torch.Generator(device=dev).manual_seed(3)
+    img = torch.randn((1, C, N, N, N), dtype=torch.complex64, device=dev, generator=g)
+    nf = b200_nufft((N, N, N), oversamp=1.25, width=4)
+    t0 = time.perf_counter()
+    k = nf.forward(img, trj)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    nf.adjoint(k, trj)
+    plan = nf._plans.entries[-1][2]
+    torch.cuda.synchronize()
+    plan.enable_timing(True)
+    plan.timing()
+    e0, e1 = _events(torch)
+    e0.record()
+    for _ in range(steps):
+        k = nf.forward(img, trj)
+        nf.adjoint(k, trj)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    st = plan.timing()
+    plan.enable_timing(False)
+    Gos = int(math.ceil(1.25 * N)) ** 3
+    alg = 8 * C * (M + Gos) + 4 * 3 * M
+    g_ms = st["grid"][0] / max(1, st["grid"][1])
+    i_ms = st["interp"][0] / max(1, st["interp"][1])
+    # autograd: loss = ||A x - y||^2, gradients for the image and the trajectory
+    x = img.clone().requires_grad_(True)
+    tr = trj.clone().requires_grad_(True)
+    y = (k * 0.9).detach()
+    for _ in range(2):
+        loss = (nf.forward(x, tr) - y).abs().square().sum()
+        loss.backward()
+    torch.cuda.synchronize()
+    e0.record()
+    loss = (nf.forward(x, tr) - y).abs().square().sum()
+    loss.backward()
+    e1.record()
+    torch.cuda.synchronize()
+    ag_ms = e0.elapsed_time(e1)
+    stats = plan.stats()
+    return {
+        "workload": "3D KB NUFFT fwd+adj: 192^3 c64, 16 coils, kooshball 20000x384, os 1.25, W 4",
+        "value": C * M / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": ms, "steps": steps,
+        "stage_ms": {k2: v[0] / steps for k2, v in st.items() if v[1]},
+        "grid_roofline": {"bound": "hbm", "algorithmic_bytes": alg, "kernel_ms": g_ms,
+                          "achieved": alg / (g_ms / 1e3) / 1e9, "peak": peak,
+                          "frac": alg / (g_ms / 1e3) / 1e9 / peak, "unit": "GB/s"},
+        "interp_roofline": {"achieved": alg / (i_ms / 1e3) / 1e9, "frac": alg / (i_ms / 1e3) / 1e9 / peak,
+                            "kernel_ms": i_ms},
+        "autograd_step_ms": ag_ms, "plan_setup_s": setup_s, "plan": stats,
+    }
+
+
+def bench_c4(dev, iters=30, seed=4, n_slices=64):
+    """Batched uneven CG-SENSE: 64 slices (matrix from {160..256}^2, 8-32
+    coils, 10k-100k spiral samples), 30 iterations captured in one CUDA graph
+    with autotuned bins/tiles, against a loop of per-slice solves on the same
+    kernels. Per-slice eigenvalue normalisation (recons.py:117-123) is folded
+    into the coil maps: A_s / sqrt(l_s)."""
+    import torch
+    from mr_recon_b200 import synth
+    from mr_recon_b200.algs import SenseCG
+    from mr_recon_b200.autotune import autotune
+    from mr_recon_b200.plan import Plan
+    rng = np.random.RandomState(seed)
+    sizes = rng.choice([160, 192, 224, 256], n_slices)
+    coils = rng.randint(8, 33, n_slices)
+    npts = rng.randint(10000, 100001, n_slices) // 16 * 16
+    xs, mps, trjs = [], [], []
+    for s in range(n_slices):
+        N = int(sizes[s])
+        xs.append(synth.ellipse_phantom((N, N), 20, rng).astype(np.complex64).reshape(-1))
+        mps.append(synth.gaussian_coil_maps((N, N), int(coils[s])).astype(np.complex64).reshape(-1))
+        trjs.append(synth.vd_spiral(16, int(npts[s]) // 16, N / 2.0).reshape(-1, 2))
+    ims = [(int(n), int(n)) for n in sizes]
+    x_t = torch.from_numpy(np.concatenate(xs)).to(dev)
+    m_t = torch.from_numpy(np.concatenate(mps)).to(dev)
+    t_t = torch.from_numpy(np.concatenate(trjs)).to(dev)
+    plan = Plan(ims, [int(m) for m in npts], [int(c) for c in coils], 1.25, (6.0, 6.0), device=dev)
+    t0 = time.perf_counter()
+    tune = autotune(plan, t_t)
+    tune_s = time.perf_counter() - t0
+    ksp = torch.empty(plan.n_ksp, dtype=torch.complex64, device=dev)
+    plan.sense_forward(x_t, m_t, ksp)
+    g = torch.Generator(device=dev).manual_seed(seed)
+    noise = torch.randn(ksp.shape, dtype=torch.complex64, device=dev, generator=g)
+    ksp += noise * (ksp.abs().square().mean().sqrt() * 10 ** (-30 / 20))
+    # per-slice max eigenvalue (batched power method, setup) folded into the maps
+    img_off = [int(o) for o in plan.img_off]
+    nimg = [int(c) * n[0] * n[1] for c, n in zip(coils, ims)]
+    xoff = np.concatenate([[0], np.cumsum([n[0] * n[1] for n in ims])])
+    v = torch.randn(int(xoff[-1]), dtype=torch.complex64, device=dev, generator=g)
+    z = torch.empty_like(v)
+    lam = None
+    for _ in range(15):
+        plan.sense_normal(v, m_t, None, z)
+        lam = torch.stack([z[xoff[s]:xoff[s + 1]].norm() for s in range(n_slices)])
+        v = z / torch.repeat_interleave(lam, torch.tensor(np.diff(xoff), device=dev))
+    lam = (lam * 1.01).double()
+    m_s = m_t.clone()
+    for s in range(n_slices):
+        m_s[img_off[s]:img_off[s] + nimg[s]] /= float(lam[s].sqrt())
+    solver = SenseCG(plan, m_s, None, iters, 1e-3, 1.0)
+    solver.ksp.copy_(ksp)
+    solver.solve()
+    solver.capture()
+    xb = solver.solve().clone()
+    torch.cuda.synchronize()
+    e0, e1 = _events(torch)
+    reps = 5
+    e0.record()
+    for _ in range(reps):
+        solver.graph.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    b_ms = e0.elapsed_time(e1) / reps
+    # per-slice loop on the same kernels: one plan and one eager solve per slice
+    ksp_off = [int(o) for o in plan.ksp_off]
+    singles = []
+    for s in range(n_slices):
+        p1 = Plan([ims[s]], [int(npts[s])], [int(coils[s])], 1.25, (6.0, 6.0), device=dev)
+        p1.set_traj(t_t[int(plan.trj_off[s]) // 2:int(plan.trj_off[s]) // 2 + int(npts[s])])
+        s1 = SenseCG(p1, m_s[img_off[s]:img_off[s] + nimg[s]], None, iters, 1e-3, 1.0)
+        s1.ksp.copy_(ksp[ksp_off[s]:ksp_off[s] + int(coils[s]) * int(npts[s])])
+        singles.append(s1)
+    for s1 in singles:
+        s1.solve()
+    torch.cuda.synchronize()
+    e0.record()
+    xs_loop = [s1.solve().clone() for s1 in singles]
+    e1.record()
+    torch.cuda.synchronize()
+    l_ms = e0.elapsed_time(e1)
+    xl = torch.cat(xs_loop)
+    return {
+        "workload": "batched uneven CG-SENSE: 64 slices, N in {160..256}^2, 8-32 coils, 10k-100k spiral "
+                    "samples, 30 iterations, lambda 1e-3",
+        "slice_solves_per_s_batched_graph": n_slices * 1e3 / b_ms, "ms_per_batch_graph": b_ms,
+        "slice_solves_per_s_per_slice_loop": n_slices * 1e3 / l_ms, "ms_per_slice_loop": l_ms,
+        "speedup": l_ms / b_ms, "batched_vs_loop_rel_diff": float((xb - xl).norm() / xl.norm()),
+        "autotune": {k: v for k, v in tune.items()}, "autotune_s": tune_s,
+        "total_coil_samples": int(sum(int(c) * int(m) for c, m in zip(coils, npts))),
+    }
+
+
 def run_reference(args, rank):
     """--impl reference: the CPU oracle port of the reference path on the host
     cores, rank 0 only; each step is a bounded sample (a few coils)."""
@@ -170,6 +331,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cg", action="store_true")
+    ap.add_argument("--extra", default="", help="comma list of extra workloads: c3 (3D), c4 (batched CG)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -330,6 +492,14 @@ def main():
                "sample": "8 of 32 coils (one per thread), full 98304-sample spiral, fwd+adj, 2 repeats",
                "seconds": secs}
 
+    extra = {}
+    if rank == 0 and world == 1:
+        want = [e.strip() for e in args.extra.split(",") if e.strip()]
+        if "c3" in want:
+            extra["c3"] = bench_c3(dev, 5, peak)
+        if "c4" in want:
+            extra["c4"] = bench_c4(dev)
+
     launches_per_step = 4 + (1 if stats["split_tiles"] > 0 else 0)
     if rank == 0:
         line = {
@@ -342,6 +512,7 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "cg_sense": cg,
             "gpu_launches": launches_per_step * args.steps, "clocks": clocks,
         }
+        line.update(extra)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -696,7 +696,9 @@ k_interp_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, K
 //     tile's cells (zero outside the kernel support and the tile): thread
 //     (entry, dimension, half) evaluates 4 cells and stores them at once;
 //   * batch b accumulates: per entry, each of the warp's tile rows with a
-//     non-zero weight takes 2 x 8 FMAs per lane.
+//     non-zero weight takes 8 packed two-lane FMAs per lane (fma.rn.f32x2:
+//     real and imaginary part of a cell in one instruction); the scale is
+//     folded into the row weights.
 // With at most 16 coils per group a warp runs SUB = 32 / CW entry streams of
 // CW lanes (CW = coil group rounded up to a power of two); their partial
 // tiles are summed with shuffles before the write-back.
@@ -731,7 +733,8 @@ k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBP
   constexpr int T = kRegTile, R = kRegRows, B = kRegBatch, CW = 32 / SUB;
   __shared__ float4 s_c[3][B];      // coordinate ring
   __shared__ int s_pm[3][B];        // sample index ring
-  __shared__ float4 s_w[2][B][4];   // per entry: row weights (cells 0-7), column weights (cells 0-7)
+  __shared__ float4 s_wr[2][B][2];  // per entry: row weights x scale (cells 0-7)
+  __shared__ float4 s_wc[2][B][4];  // per entry: column weights, each twice (cells 0-7)
   __shared__ float2 s_v[2][B][CW];  // per entry and coil: sample value
   __shared__ float s_d[2][B];       // per entry: density weight
   __shared__ float2 s_t[2][B];      // per entry: temporal weight
@@ -766,10 +769,8 @@ k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBP
       for (int j = sid; j < nb; j += 2 * SUB) cp_async8(&s_v[b2][j][coil], kspc + (s_pm[r3][j] - pt_off));
     if (tid < nb) {
       if (dcf) cp_async4(&s_d[b2][tid], dcf + s_pm[r3][tid]);
-      else s_d[b2][tid] = 1.f;
     } else if (tid >= 32 && tid - 32 < nb) {
       if (temporal) cp_async8(&s_t[b2][tid - 32], temporal + s_pm[r3][tid - 32]);
-      else s_t[b2][tid - 32] = make_float2(1.f, 0.f);
     }
   };
   // tile-aligned 1D weights of batch bi: thread = (entry, dimension, half of the cells)
@@ -793,7 +794,12 @@ k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBP
       const float adx = fabsf(__fsub_rn((float)(lo + q), u));
       w[l] = (q >= 0 && q < K && cell < size && adx <= r) ? kb_tap_fast(adx, ir, kb.beta) : 0.f;
     }
-    s_w[bi & 1][j][2 * i + h] = make_float4(w[0], w[1], w[2], w[3]);
+    if (i == 0) {
+      s_wr[bi & 1][j][h] = make_float4(w[0] * scale, w[1] * scale, w[2] * scale, w[3] * scale);
+    } else {
+      s_wc[bi & 1][j][2 * h] = make_float4(w[0], w[0], w[1], w[1]);
+      s_wc[bi & 1][j][2 * h + 1] = make_float4(w[2], w[2], w[3], w[3]);
+    }
   };
 
   float2 acc[R][T];
@@ -822,24 +828,30 @@ k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBP
     weights(bi + 1);
     const int b2 = bi & 1, nb = batch_len(bi);
     for (int j = sub; j < nb; j += SUB) {
-      const float4 rw = s_w[b2][j][warp];
-      const float4 q0 = s_w[b2][j][2], q1 = s_w[b2][j][3];
+      const float4 rw = s_wr[b2][j][warp];
       const float wr[R] = {rw.x, rw.y, rw.z, rw.w};
-      const float wc[T] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-      const float hs = scale * s_d[b2][j];
-      const float2 t = s_t[b2][j];
-      const float2 hh = make_float2(hs * t.x, -hs * t.y);
-      const float2 a0 = s_v[b2][j][coil];
-      const float2 val = make_float2(a0.x * hh.x - a0.y * hh.y, a0.x * hh.y + a0.y * hh.x);
+      float2 wc[T];
+#pragma unroll
+      for (int b = 0; b < T / 2; ++b) {
+        const float4 c = s_wc[b2][j][b];
+        wc[2 * b] = make_float2(c.x, c.y);
+        wc[2 * b + 1] = make_float2(c.z, c.w);
+      }
+      float2 val = s_v[b2][j][coil];
+      if (dcf) {
+        const float d = s_d[b2][j];
+        val = make_float2(val.x * d, val.y * d);
+      }
+      if (temporal) {  // times conj(t)
+        const float2 t = s_t[b2][j];
+        val = make_float2(val.x * t.x + val.y * t.y, val.y * t.x - val.x * t.y);
+      }
 #pragma unroll
       for (int a = 0; a < R; ++a) {
         if (SUB == 1 && wr[a] == 0.f) continue;  // uniform: one entry per warp
-        const float vx = wr[a] * val.x, vy = wr[a] * val.y;
+        const float2 v2 = make_float2(wr[a] * val.x, wr[a] * val.y);
 #pragma unroll
-        for (int b = 0; b < T; ++b) {
-          acc[a][b].x = fmaf(wc[b], vx, acc[a][b].x);
-          acc[a][b].y = fmaf(wc[b], vy, acc[a][b].y);
-        }
+        for (int b = 0; b < T; ++b) acc[a][b] = __ffma2_rn(wc[b], v2, acc[a][b]);  // both lanes of the cell
       }
     }
   }

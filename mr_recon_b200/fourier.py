@@ -153,8 +153,9 @@ class b200_nufft(NUFFT):
                  beta: Optional[float] = None, apodize: Optional[bool] = True,
                  tile: Optional[tuple] = None, coil_group: int = 0, max_chunk: int = 0,
                  fast: bool = True, warp_grid: bool = True, weight_tables: bool = False,
-                 reg_grid: bool = True, reg_interp: bool = True):
+                 reg_grid: bool = True, reg_interp: bool = True, autotune: bool = False):
         super().__init__(im_size)
+        self.autotune = autotune
         self.fast = fast
         self.reg_grid = reg_grid
         self.reg_interp = reg_interp
@@ -190,7 +191,11 @@ class b200_nufft(NUFFT):
                      warp_grid=self.warp_grid, weight_tables=self.weight_tables,
                      reg_grid=self.reg_grid, reg_interp=self.reg_interp)
             if trj is not None and M > 0:
-                p.set_traj(trj)
+                if self.autotune:
+                    from .autotune import autotune
+                    autotune(p, trj.detach().to(torch.float32).contiguous())
+                else:
+                    p.set_traj(trj)
             return p
 
         return self._plans.get(key, trj, make)

@@ -110,7 +110,11 @@ class sense_linop(linop):
                              max_chunk=nufft.max_chunk, device=dev, fast=nufft.fast,
                              warp_grid=nufft.warp_grid, weight_tables=nufft.weight_tables,
                              reg_grid=nufft.reg_grid, reg_interp=nufft.reg_interp)
-            self.plan.set_traj(trj.contiguous())
+            if getattr(nufft, "autotune", False):
+                from .autotune import autotune
+                autotune(self.plan, trj.contiguous())
+            else:
+                self.plan.set_traj(trj.contiguous())
 
         if use_toeplitz:
             # linops.py:1102-1119: the spatial/temporal defaults are already in

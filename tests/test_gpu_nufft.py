@@ -231,6 +231,31 @@ def test_plan_decomposition_options_rebind(opts):
     assert rel(Nn(out).reshape(1, C, *im), on.adjoint(y[None], trj[None])) < TOL
 
 
+def test_autotune_keeps_parity_and_caches():
+    """The autotuner times candidate decompositions on the bound trajectory,
+    leaves the plan bound with the fastest, and reuses the choice for the
+    same geometry without timing."""
+    from mr_recon_b200 import autotune as AT
+    AT.clear_cache()
+    rng = np.random.RandomState(21)
+    im, C = (72, 64), 7
+    trj = synth.vd_spiral(6, 800, 32.0).reshape(1, -1, 2)
+    img = synth.randn_complex((1, C, *im), rng)
+    y = synth.randn_complex((1, C, trj.shape[1]), rng)
+    on = O.KBNufftOracle(im, 1.25, 6)
+    nf = b200_nufft(im, oversamp=1.25, width=6, autotune=True)
+    assert rel(Nn(nf.forward(T(img), T(trj))), on.forward(img, trj)) < TOL
+    assert rel(Nn(nf.adjoint(T(y), T(trj))), on.adjoint(y, trj)) < TOL
+    plan = nf._plans.entries[-1][2]
+    cand = AT.default_candidates(2)
+    res = AT.autotune(plan, T(trj.reshape(-1, 2)))
+    assert res["cached"]
+    assert res["interp_tile"] in cand["interp_tile"] and res["grid_chunk"] in cand["grid_chunk"]
+    ksp = torch.empty(C * trj.shape[1], dtype=torch.complex64, device=DEV)
+    plan.forward(T(img).reshape(-1), ksp)
+    assert rel(Nn(ksp).reshape(1, C, -1), on.forward(img, trj)) < TOL
+
+
 @pytest.mark.parametrize("tile", [(8, 8), (16, 32), (64, 64), (5, 7)])
 def test_tile_shapes_agree(tile):
     rng = np.random.RandomState(11)
