@@ -794,6 +794,8 @@ int launch_grid_t(mrn_plan* P, const float2* ksp, const float* dcf, const float2
       k_zero_split<3><<<nb, 256, 0, st>>>(P->d_split_tiles, P->d_counts, P->d_slices, P->nslices, grid, (int)layout);
   }
   dim3 gridDim((unsigned)P->n_items_grid, (unsigned)((P->max_coil + L.cg - 1) / L.cg));
+  if (fast && P->ndim == 3 && grid_reg3_ok(P))
+    return launch_grid_reg3(P, ksp, dcf, temporal, (int)layout, grid, scale, st);
   if (fast && P->ndim == 2 && P->warp_grid && grid_reg_ok(P))
     return launch_grid_reg(P, ksp, dcf, temporal, (int)layout, grid, scale, st);
   if (fast && P->ndim == 2 && P->warp_grid && P->wtab_ok && P->use_wtab)
