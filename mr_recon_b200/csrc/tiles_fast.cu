@@ -908,7 +908,7 @@ k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBP
 // accumulation in a fixed order.
 // ---------------------------------------------------------------------------
 constexpr int kReg3Tile = 8;
-constexpr int kReg3Batch = 16;
+constexpr int kReg3Batch = 32;
 constexpr int kReg3Coils = 16;
 
 template <int K>
@@ -948,18 +948,20 @@ k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
     if (tid < nb) cp_async16(&s_c[r3][tid], coord + it.start + bi * B + tid);
     else if (tid >= 32 && tid - 32 < nb) cp_async4(&s_pm[r3][tid - 32], perm + it.start + bi * B + tid - 32);
   };
-  // thread = (entry j, coil c): one 8-byte copy each
+  // thread = (entry j and j + 16, coil c): one 8-byte copy per entry and coil
   auto copy_values = [&](int bi) {
     const int nb = batch_len(bi), b2 = bi & 1, r3 = bi % 3;
-    const int j = tid >> 4, c = tid & 15;
-    if (j < nb && c < ncg) cp_async8(&s_v[b2][j][c], kspg + (int64_t)c * m + (s_pm[r3][j] - pt_off));
+    const int c = tid & 15;
+#pragma unroll
+    for (int j = tid >> 4; j < B; j += 16)
+      if (j < nb && c < ncg) cp_async8(&s_v[b2][j][c], kspg + (int64_t)c * m + (s_pm[r3][j] - pt_off));
     if (tid < nb) {
       if (dcf) cp_async4(&s_d[b2][tid], dcf + s_pm[r3][tid]);
     } else if (tid >= 32 && tid - 32 < nb) {
       if (temporal) cp_async8(&s_t[b2][tid - 32], temporal + s_pm[r3][tid - 32]);
     }
   };
-  // thread < 96 = (entry j, dimension i, half hh): tile-aligned weights of 4 cells
+  // thread < 6 B = (entry j, dimension i, half hh): tile-aligned weights of 4 cells
   auto weights = [&](int bi) {
     if (tid >= 6 * B) return;
     const int pair = tid >> 1, hh = tid & 1;
