@@ -102,7 +102,7 @@ int mrn_plan_stats(mrn_plan* plan, int64_t* out4);
  * MRN_OPT_INTERP_CHUNK / MRN_OPT_GRID_CHUNK: samples per interpolation work
  * item and gridding entries per gridding work item (defaults: 256 / 256 in
  * 2D, 1024 otherwise); MRN_OPT_INTERP_TILE / MRN_OPT_GRID_TILE: tile edge in
- * grid cells, every dimension (defaults: 10 / 8 in 2D, 8 in 3D, 256 in 1D). */
+ * grid cells, every dimension (defaults: 10 / 8 in 2D, 6 / 8 in 3D, 256 in 1D). */
 #define MRN_OPT_INTERP_CHUNK 4
 #define MRN_OPT_GRID_CHUNK 5
 #define MRN_OPT_INTERP_TILE 6
@@ -111,9 +111,9 @@ int mrn_plan_stats(mrn_plan* plan, int64_t* out4);
  * keep their accumulator in registers (two warps per tile, lane = coil);
  * 0 keeps it in shared memory. Both sum in the same fixed order. */
 #define MRN_OPT_REG_GRIDDING 8
-/* MRN_OPT_REG_INTERP (default 1): 2D interpolation with one lane per coil
- * over the tile region staged as [cell][coil] (packed two-lane FMAs); 0 uses
- * the coil-plane kernel. */
+/* MRN_OPT_REG_INTERP (default 1): 2D and 3D interpolation with one lane per
+ * coil over the tile region staged as [cell][coil] (packed two-lane FMAs); 0
+ * uses the coil-plane kernel. */
 #define MRN_OPT_REG_INTERP 9
 int mrn_plan_set_option(mrn_plan* plan, int option, int value);
 

@@ -394,12 +394,12 @@ int mrn_plan_create(mrn_plan** out, int ndim, int n_slices, const int* im_size,
   P->max_coil = maxc;
 
   // Built-in interpolation tile: 10 cells per edge in 2D (tile + halo as a [cell][coil]
-  // region for 32 coils: three CTAs per SM), 8 in 3D, 256 in 1D.
+  // region for 32 coils: three CTAs per SM), 6 in 3D (8-coil groups), 256 in 1D.
   int deftile[kMaxDim];
-  for (int i = 0; i < ndim; ++i) deftile[i] = (ndim == 1) ? 256 : (ndim == 2 ? 10 : 8);
+  for (int i = 0; i < ndim; ++i) deftile[i] = (ndim == 1) ? 256 : (ndim == 2 ? 10 : 6);
   for (int i = 0; i < ndim; ++i) P->tile[i] = tile ? tile[i] : deftile[i];
   // gridding tiles: 8x8 in 2D (one warp owns a tile), else the interpolation tile
-  for (int i = 0; i < ndim; ++i) P->gtile[i] = (ndim == 2 && !tile) ? 8 : P->tile[i];
+  for (int i = 0; i < ndim; ++i) P->gtile[i] = (ndim >= 2 && !tile) ? 8 : P->tile[i];
   P->max_chunk = max_chunk > 0 ? max_chunk : (ndim == 2 ? 256 : 1024);
   // one warp grids a 2D tile item alone: shorter items keep warps balanced
   P->grid_chunk = max_chunk > 0 ? max_chunk : (ndim == 2 ? 256 : 1024);

@@ -61,6 +61,13 @@ __device__ __forceinline__ int wrap_once(int a, int n) {
 template <class T>
 __device__ __forceinline__ T sel3(const T* v, int i) { return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]); }
 
+// a mod n for a in (-n, inf), by subtraction (region rows may wrap more than once on tiny grids)
+__device__ __forceinline__ int wrap_cells(int a, int n) {
+  a = a < 0 ? a + n : a;
+  while (a >= n) a -= n;
+  return a;
+}
+
 // 1D weights of one sample, w[i][q] for dim i, tap q (0 when invalid). The G
 // lanes of a slot compute the D*K entries round-robin and exchange them by
 // shuffles. With OWN, taps whose local cell st[i] + q lies outside [0,
@@ -557,21 +564,21 @@ k_grid_warp(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
 }
 
 // ---------------------------------------------------------------------------
-// 2D interpolation, lane = coil. The CTA stages its tile region (tile + K-1
-// halo, wrapped) for up to 32 coils in shared memory as [cell][coil] with an
-// odd coil stride CS = CW + 1: the transposing load writes without bank
-// conflicts and a warp reading one cell for all its coils touches
-// consecutive words. Each warp then takes one sample at a time (SUB samples
-// when the coil group is at most 16 / 8 wide): the 2K 1D weights are
-// computed once by the sample's lanes and broadcast with shuffles, and each
-// lane sums its coil's K x K taps row by row with packed two-lane FMAs
+// 2D / 3D interpolation, lane = coil. The CTA stages its tile region (tile +
+// K-1 halo, wrapped) for a group of coils in shared memory as [cell][coil]
+// with an odd coil stride CS = CW + 1: the transposing load writes without
+// bank conflicts and lanes reading one cell for all their coils touch
+// consecutive words. Each warp then takes SUB samples at a time (one per
+// group of CW = 32 / SUB lanes): the d*K 1D weights of a sample are computed
+// once by its lanes and broadcast with shuffles, and each lane sums its
+// coil's K^d taps along the last axis with packed two-lane FMAs
 // (fma.rn.f32x2: real and imaginary part in one instruction), one shared
-// load per tap.
+// load per tap, then combines the rows with the outer weights.
 // ---------------------------------------------------------------------------
 constexpr int kRegInterpWarps = 8;
 constexpr int kInterpStage = 256;  // samples whose coordinates are staged at once
 
-template <int K, int SUB>
+template <int D, int K, int SUB>
 __global__ void __launch_bounds__(kRegInterpWarps * 32)
 k_interp_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBParams kb,
              const float4* __restrict__ coord, const int* __restrict__ perm,
@@ -580,7 +587,7 @@ k_interp_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, K
   constexpr int CW = 32 / SUB, CS = CW + 1, NW = kRegInterpWarps, NT = NW * 32;
   extern __shared__ float4 smem_f4[];
   float2* region = reinterpret_cast<float2*>(smem_f4);
-  __shared__ float2 s_u[kInterpStage];  // coordinates of the staged samples
+  __shared__ float4 s_u[kInterpStage];  // coordinates of the staged samples
   __shared__ int s_p[kInterpStage];     // their sample indices within the slice
 
   const Item it = items[blockIdx.x];
@@ -589,11 +596,15 @@ k_interp_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, K
   const int c0 = blockIdx.y * cg;
   if (c0 >= ncoil) return;
   const int ncg = min(cg, ncoil - c0);
-  const int nos0 = gp->nos[0], nos1 = gp->nos[1];
-  const int hs0 = layout == kInternal ? gp->hshift[0] : 0;
-  const int hs1 = layout == kInternal ? gp->hshift[1] : 0;
-  const Frame f = frame_of(*gp, it.tile, 2, false);
-  const int ext0 = f.size[0] + K - 1, ext1 = f.size[1] + K - 1;
+  int nos[3], hs[3], ext[3];
+  const Frame f = frame_of(*gp, it.tile, D, false);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    nos[i] = gp->nos[i];
+    hs[i] = (i < D && layout == kInternal) ? gp->hshift[i] : 0;
+    ext[i] = i < D ? f.size[i] + K - 1 : 1;
+  }
+  const int inner = ext[D - 1];
   const int64_t gos = gp->gos;
   const float2* gbase = grid + (layout == kInternal ? gp->grid_off : gp->ugrid_off) + (int64_t)c0 * gos;
   const int64_t m = gp->m, pt_off = gp->pt_off;
@@ -606,21 +617,30 @@ k_interp_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, K
     const int ns = min(kInterpStage, it.count - sb);
     if (sb > 0) __syncthreads();  // every warp is done with the previous stage
     for (int j = tid; j < ns; j += NT) {
-      const float4 c4 = coord[it.start + sb + j];
-      s_u[j] = make_float2(c4.x, c4.y);
+      s_u[j] = coord[it.start + sb + j];
       s_p[j] = (int)(perm[it.start + sb + j] - pt_off);
     }
     if (sb == 0) {
-      // region: thread = one cell (r, q), looping over the coil planes with
-      // the global address stepped by the plane stride; kLoadBatch loads in
+      // region: thread = one cell, looping over the coil planes with the
+      // global address stepped by the plane stride; kLoadBatch loads in
       // flight per thread. Consecutive threads read consecutive cells of a
       // row and write shared words 2 * CS apart (CS odd: no bank conflict).
       constexpr int kLoadBatch = 8;
-      for (int cell = tid; cell < ext0 * ext1; cell += NT) {
-        const int r = cell / ext1, q = cell - r * ext1;
-        int s = wrap_once(f.org[1] - hs1, nos1) + q;
-        while (s >= nos1) s -= nos1;
-        const float2* src = gbase + (int64_t)wrap_once(f.org[0] + r - hs0, nos0) * nos1 + s;
+      const int ncells = ext[0] * ext[1] * ext[2];
+      for (int cell = tid; cell < ncells; cell += NT) {
+        int64_t off;
+        if (D == 2) {
+          const int r = cell / inner, q = cell - r * inner;
+          off = (int64_t)wrap_cells(f.org[0] + r - hs[0], nos[0]) * nos[1] +
+                wrap_cells(f.org[1] + q - hs[1], nos[1]);
+        } else {
+          const int rz = cell / inner, z = cell - rz * inner;
+          const int x = rz / ext[1], y = rz - x * ext[1];
+          off = ((int64_t)wrap_cells(f.org[0] + x - hs[0], nos[0]) * nos[1] +
+                 wrap_cells(f.org[1] + y - hs[1], nos[1])) * nos[2] +
+                wrap_cells(f.org[2] + z - hs[2], nos[2]);
+        }
+        const float2* src = gbase + off;
         float2* dst = region + cell * CS;
         for (int cb = 0; cb < ncg; cb += kLoadBatch) {
           float2 v[kLoadBatch];
@@ -638,27 +658,47 @@ k_interp_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, K
     for (int base = warp * SUB; base < ns; base += NW * SUB) {
       const int el = base + sub;
       const bool active = el < ns;
-      const float2 uu = s_u[active ? el : base];
-      const float u[3] = {uu.x, uu.y, 0.f};
+      const float4 uu = s_u[active ? el : base];
+      const float u[3] = {uu.x, uu.y, uu.z};
       int lo[3] = {0, 0, 0}, l0[3] = {0, 0, 0};
 #pragma unroll
-      for (int i = 0; i < 2; ++i) {
+      for (int i = 0; i < D; ++i) {
         lo[i] = (int)ceilf(__fsub_rn(u[i], kb.radius[i]));
-        l0[i] = wrap_once(lo[i], i == 0 ? nos0 : nos1) - f.org[i];
+        l0[i] = wrap_once(lo[i], nos[i]) - f.org[i];
       }
-      float w[2][K];
-      sample_weights<2, K, CW, false>(u, lo, l0, f.size, kb, lane, w);
+      float w[D][K];
+      sample_weights<D, K, CW, false>(u, lo, l0, f.size, kb, lane, w);
       if (!active || !has_coil) continue;
-      const float2* rb = region + (l0[0] * ext1 + l0[1]) * CS + coil;
+      float2 wl[K];  // last-axis weights, each twice
+#pragma unroll
+      for (int b = 0; b < K; ++b) wl[b] = make_float2(w[D - 1][b], w[D - 1][b]);
       float2 acc = make_float2(0.f, 0.f);
+      if (D == 2) {
+        const float2* rb = region + (l0[0] * inner + l0[1]) * CS + coil;
 #pragma unroll
-      for (int a = 0; a < K; ++a) {
-        if (w[0][a] == 0.f) continue;
-        const float2* rp = rb + a * ext1 * CS;
-        float2 ra = make_float2(0.f, 0.f);
+        for (int a = 0; a < K; ++a) {
+          if (SUB == 1 && w[0][a] == 0.f) continue;
+          const float2* rp = rb + a * inner * CS;
+          float2 ra = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int b = 0; b < K; ++b) ra = __ffma2_rn(make_float2(w[1][b], w[1][b]), rp[b * CS], ra);
-        acc = __ffma2_rn(make_float2(w[0][a], w[0][a]), ra, acc);
+          for (int b = 0; b < K; ++b) ra = __ffma2_rn(wl[b], rp[b * CS], ra);
+          acc = __ffma2_rn(make_float2(w[0][a], w[0][a]), ra, acc);
+        }
+      } else {
+        const float2* rb = region + ((l0[0] * ext[1] + l0[1]) * inner + l0[D - 1]) * CS + coil;
+#pragma unroll
+        for (int a = 0; a < K; ++a) {
+          float2 pa = make_float2(0.f, 0.f);
+#pragma unroll
+          for (int b = 0; b < K; ++b) {
+            const float2* rp = rb + (a * ext[1] + b) * inner * CS;
+            float2 ra = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int c = 0; c < K; ++c) ra = __ffma2_rn(wl[c], rp[c * CS], ra);
+            pa = __ffma2_rn(make_float2(w[D > 2 ? 1 : 0][b], w[D > 2 ? 1 : 0][b]), ra, pa);
+          }
+          acc = __ffma2_rn(make_float2(w[0][a], w[0][a]), pa, acc);
+        }
       }
       const int lp = s_p[el];
       float2 h = make_float2(scale, 0.f);
@@ -1180,8 +1220,12 @@ int launch_grid_warp(mrn_plan* P, const float2* ksp, const float* dcf, const flo
   return e == cudaSuccess ? MRN_OK : cuda_fail(e);
 }
 
+// Coil group of the lane-per-coil interpolation: all coils of the widest
+// slice up to 32 lanes (2D) or 8 (3D: a 6^3 tile region with its halo then
+// fits three CTAs per SM), or the caller's coil_group.
 static int interp_reg_sub(const mrn_plan* P, int* cg_out, int* ng_out) {
-  int cg = P->coil_group_req > 0 ? std::min(P->coil_group_req, P->max_coil) : P->max_coil;
+  const int cap = P->ndim == 3 ? 8 : 32;
+  int cg = P->coil_group_req > 0 ? std::min(P->coil_group_req, P->max_coil) : std::min(P->max_coil, cap);
   cg = std::max(1, std::min(cg, 32));
   const int ng = (P->max_coil + cg - 1) / cg;
   cg = (P->max_coil + ng - 1) / ng;
@@ -1192,14 +1236,16 @@ static int interp_reg_sub(const mrn_plan* P, int* cg_out, int* ng_out) {
 
 static size_t interp_reg_smem(const mrn_plan* P, int sub) {
   const int K = P->kb.ntaps[0];
-  return (size_t)(P->tmax_cells[0] + K - 1) * (P->tmax_cells[1] + K - 1) * (32 / sub + 1) * sizeof(float2);
+  size_t cells = 1;
+  for (int i = 0; i < P->ndim; ++i) cells *= (size_t)(P->tmax_cells[i] + K - 1);
+  return cells * (32 / sub + 1) * sizeof(float2);
 }
 
 bool interp_reg_ok(const mrn_plan* P) {
-  if (!P->reg_interp || P->ndim != 2) return false;
+  if (!P->reg_interp || (P->ndim != 2 && P->ndim != 3)) return false;
   int cg, ng;
   const int sub = interp_reg_sub(P, &cg, &ng);
-  return interp_reg_smem(P, sub) + kInterpStage * (sizeof(float2) + sizeof(int)) <= 227 * 1024;
+  return interp_reg_smem(P, sub) + kInterpStage * (sizeof(float4) + sizeof(int)) <= 227 * 1024;
 }
 
 int launch_interp_reg(mrn_plan* P, const float2* grid, int layout, float2* ksp, float scale,
@@ -1211,22 +1257,26 @@ int launch_interp_reg(mrn_plan* P, const float2* grid, int layout, float2* ksp, 
   const dim3 gdim((unsigned)P->n_items_interp, (unsigned)ng);
   const int K = P->kb.ntaps[0];
   int rc = MRN_OK;
-#define MRN_IREG_LAUNCH(KK, SS)                                                                     \
+#define MRN_IREG_LAUNCH(DD, KK, SS)                                                                 \
   do {                                                                                              \
-    auto kern = k_interp_reg<KK, SS>;                                                               \
+    auto kern = k_interp_reg<DD, KK, SS>;                                                           \
     rc = prep_attr(kern, smem);                                                                     \
     if (rc == MRN_OK)                                                                               \
       kern<<<gdim, kRegInterpWarps * 32, smem, st>>>(P->d_items_i, P->d_slices, P->kb, P->d_coord_i, \
                                                      P->d_perm_i, grid, layout, ksp, scale, temporal, cg); \
   } while (0)
-#define MRN_IREG_SUB(KK)                     \
-  if (sub == 4) MRN_IREG_LAUNCH(KK, 4);      \
-  else if (sub == 2) MRN_IREG_LAUNCH(KK, 2); \
-  else MRN_IREG_LAUNCH(KK, 1)
-  if (K == 5) { MRN_IREG_SUB(5); }
-  else if (K == 6) { MRN_IREG_SUB(6); }
-  else if (K == 7) { MRN_IREG_SUB(7); }
-  else { MRN_IREG_SUB(8); }
+#define MRN_IREG_SUB(DD, KK)                     \
+  if (sub == 4) MRN_IREG_LAUNCH(DD, KK, 4);      \
+  else if (sub == 2) MRN_IREG_LAUNCH(DD, KK, 2); \
+  else MRN_IREG_LAUNCH(DD, KK, 1)
+#define MRN_IREG_K(DD)                      \
+  if (K == 5) { MRN_IREG_SUB(DD, 5); }      \
+  else if (K == 6) { MRN_IREG_SUB(DD, 6); } \
+  else if (K == 7) { MRN_IREG_SUB(DD, 7); } \
+  else { MRN_IREG_SUB(DD, 8); }
+  if (P->ndim == 2) { MRN_IREG_K(2) }
+  else { MRN_IREG_K(3) }
+#undef MRN_IREG_K
 #undef MRN_IREG_SUB
 #undef MRN_IREG_LAUNCH
   if (rc != MRN_OK) return rc;
