@@ -54,17 +54,23 @@ struct Item {
   int pad[3];
 };
 
+constexpr int kKBTerms = 32;  // terms of the I0 power series kept in KBParams
+
 struct KBParams {
   float radius[kMaxDim];  // W_i / 2
   float beta;
   int ntaps[kMaxDim];     // candidate taps floor(W_i) + 1
   float inv_radius[kMaxDim];  // 1 / (W_i / 2)
+  int series;             // 1: coef holds the series below to float32 accuracy for this beta
+  float coef[kKBTerms];   // (beta^2 / 4)^k / (k!)^2, k = 0 .. kKBTerms-1
 };
 
 // Tap weight from |dx| with a precomputed 1/r (the validity test |dx| <= r is
-// done by the caller in float32, exactly as the reference's mask); differs
-// from kb_tap only by the rounding of |dx|/r vs |dx|*(1/r) (<= 1 ulp).
-__device__ __forceinline__ float kb_tap_fast(float adx, float inv_r, float beta) {
+// done by the caller in float32, exactly as the reference's mask), by the
+// Abramowitz & Stegun polynomial approximations of I0 (the reference's
+// kernel, kernels.py:180-246); differs from kb_tap only by the rounding of
+// |dx|/r vs |dx|*(1/r) (<= 1 ulp).
+__device__ __forceinline__ float kb_tap_as(float adx, float inv_r, float beta) {
   const float x = adx * inv_r;
   const float z = beta * sqrtf(fmaxf(1.0f - x * x, 0.0f));
   if (z < 3.75f) {
@@ -77,6 +83,28 @@ __device__ __forceinline__ float kb_tap_fast(float adx, float inv_r, float beta)
                   s * (0.00916281f + s * (-0.02057706f + s * (0.02635537f +
                   s * (-0.01647633f + s * 0.00392377f)))))));
   return expf(z) * rsqrtf(z) * p;
+}
+
+// The same weight from the power series I0(z) = sum_k (z^2/4)^k / (k!)^2
+// (Abramowitz & Stegun 9.6.10) with z^2 = beta^2 t, t = 1 - x^2: a polynomial
+// in t whose coefficients are all positive, so Horner's rule in float32 has
+// no cancellation (relative error a few ulp, below the 1e-7 error of the
+// A&S approximations themselves). kKBTerms fused multiply-adds with the
+// coefficients in kernel parameter space: no branch, no special-function
+// unit, no square root.
+__device__ __forceinline__ float kb_tap_series(float adx, float inv_r, const KBParams& kb) {
+  const float x = adx * inv_r;
+  const float t = fmaxf(1.0f - x * x, 0.0f);
+  float w = kb.coef[kKBTerms - 1];
+#pragma unroll
+  for (int k = kKBTerms - 2; k >= 0; --k) w = fmaf(w, t, kb.coef[k]);
+  return w;
+}
+
+// Weight used by the fast tile kernels: the series when it converges within
+// kKBTerms terms for this beta (every beta reachable with W < 8), else A&S.
+__device__ __forceinline__ float kb_tap_fast(float adx, float inv_r, const KBParams& kb) {
+  return kb.series ? kb_tap_series(adx, inv_r, kb) : kb_tap_as(adx, inv_r, kb.beta);
 }
 
 // --------------------------------------------------------------------------

@@ -383,6 +383,20 @@ int mrn_plan_create(mrn_plan** out, int ndim, int n_slices, const int* im_size,
   }
   P->beta = beta;
   P->kb.beta = (float)beta;
+  {
+    // I0 power series in t = 1 - x^2: c_k = (beta^2/4)^k / (k!)^2, in double
+    const double q = beta * beta / 4.0;
+    double c = 1.0, sum = 0.0;
+    for (int k = 0; k < kKBTerms; ++k) {
+      P->kb.coef[k] = (float)c;
+      sum += c;
+      c *= q / ((double)(k + 1) * (k + 1));
+    }
+    // c now holds the first omitted term; later terms shrink by q / (k+1)^2 each
+    const double ratio = q / ((double)(kKBTerms + 1) * (kKBTerms + 1));
+    const double tail = ratio < 1.0 ? c / (1.0 - ratio) : 1e300;
+    P->kb.series = tail < 1e-9 * sum ? 1 : 0;
+  }
 
   int maxc = 0;
   for (int s = 0; s < n_slices; ++s) {

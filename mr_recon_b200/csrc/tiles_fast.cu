@@ -94,7 +94,7 @@ __device__ __forceinline__ void sample_weights(const float* u, const int* lo, co
         const int l = sel3(st, i) + q;
         ok = ok && l >= 0 && l < sel3(size, i);
       }
-      if (ok) v = kb_tap_fast(adx, sel3(kb.inv_radius, i), kb.beta);
+      if (ok) v = kb_tap_fast(adx, sel3(kb.inv_radius, i), kb);
     }
     mine[it] = v;
   }
@@ -576,7 +576,7 @@ k_grid_warp(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
 // load per tap, then combines the rows with the outer weights.
 // ---------------------------------------------------------------------------
 constexpr int kRegInterpWarps = 8;
-constexpr int kInterpStage = 256;  // samples whose coordinates are staged at once
+constexpr int kInterpStage = 128;  // samples whose coordinates are staged at once
 
 template <int D, int K, int SUB>
 __global__ void __launch_bounds__(kRegInterpWarps * 32)
@@ -832,7 +832,7 @@ k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBP
       const int cell = 4 * h + l;
       const int q = cell - st;
       const float adx = fabsf(__fsub_rn((float)(lo + q), u));
-      w[l] = (q >= 0 && q < K && cell < size && adx <= r) ? kb_tap_fast(adx, ir, kb.beta) : 0.f;
+      w[l] = (q >= 0 && q < K && cell < size && adx <= r) ? kb_tap_fast(adx, ir, kb) : 0.f;
     }
     if (i == 0) {
       s_wr[bi & 1][j][h] = make_float4(w[0] * scale, w[1] * scale, w[2] * scale, w[3] * scale);
@@ -1020,7 +1020,7 @@ k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
       const int cell = 4 * hh + l;
       const int q = cell - st;
       const float adx = fabsf(__fsub_rn((float)(lo + q), u));
-      w[l] = (q >= 0 && q < K && cell < size && adx <= r) ? kb_tap_fast(adx, ir, kb.beta) : 0.f;
+      w[l] = (q >= 0 && q < K && cell < size && adx <= r) ? kb_tap_fast(adx, ir, kb) : 0.f;
     }
     const int b2 = bi & 1;
     if (i == 0) {

@@ -37,7 +37,7 @@ __device__ __forceinline__ int slice_of_tile(const SliceGeom* sl, int ns, int t,
 
 // Weights of one dim for a sample at u, taps q = 0..K-1 from lo, restricted to
 // local cells [0, size) when OWN (local cell of tap q is st + q); compacted.
-__device__ __forceinline__ void dim_table(float u, float r, float inv_r, float beta, int K, int st,
+__device__ __forceinline__ void dim_table(float u, float r, float inv_r, const KBParams& kb, int K, int st,
                                           int size, bool own, int* first, int* count, float* w8) {
   const int lo = (int)ceilf(__fsub_rn(u, r));
   int q0 = -1, n = 0;
@@ -48,7 +48,7 @@ __device__ __forceinline__ void dim_table(float u, float r, float inv_r, float b
     if (own) ok = ok && (st + q) >= 0 && (st + q) < size;
     if (ok) {
       if (q0 < 0) q0 = q;
-      tmp[n++] = kb_tap_fast(adx, inv_r, beta);
+      tmp[n++] = kb_tap_fast(adx, inv_r, kb);
     }
   }
   for (int j = 0; j < 8; ++j) w8[j] = j < n ? tmp[j] : 0.f;
@@ -79,7 +79,7 @@ __global__ void k_wtab(const SliceGeom* __restrict__ sl, int ns, KBParams kb,
     const int lo = (int)ceilf(__fsub_rn(u[i], kb.radius[i]));
     int st = wrap1(lo, g.nos[i]) - org;
     if (gridding && st >= size) st -= g.nos[i];  // footprint wraps into the tile from the end
-    dim_table(u[i], kb.radius[i], kb.inv_radius[i], kb.beta, kb.ntaps[i], st, size, gridding != 0,
+    dim_table(u[i], kb.radius[i], kb.inv_radius[i], kb, kb.ntaps[i], st, size, gridding != 0,
               &first[i], &cnt[i], w[i]);
   }
   meta[e] = make_int4(first[0], first[1], cnt[0], cnt[1]);
