@@ -346,6 +346,7 @@ def main():
     from mr_recon_b200.linops import sense_linop
     from mr_recon_b200.algs import SenseCG
     from mr_recon_b200 import synth
+    from mr_recon_b200.shard import max_over_ranks
 
     if args.warmup < 3:
         args.warmup = 3
@@ -394,10 +395,7 @@ def main():
     stage = plan.timing()
     plan.enable_timing(False)
     total_ms = sum(a.elapsed_time(b) for a, b in evs)
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, dev)  # the slowest rank sets the job time
     value = world * C * M * args.steps / (total_ms / 1e3) / 1e6
 
     # roofline of the dominant kernel (gridding or interpolation)
@@ -437,10 +435,8 @@ def main():
         e2e_step()
     e1.record()
     torch.cuda.synchronize()
-    te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_val = world * C * M * ne / (float(te.item()) / 1e3) / 1e6
+    te_ms = max_over_ranks(e0.elapsed_time(e1), dev)
+    e2e_val = world * C * M * ne / (te_ms / 1e3) / 1e6
     nbytes_img = img_h.numel() * 8
     nbytes_ksp = ksp_h.numel() * 8
     e2e = {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": nbytes_img + nbytes_ksp,
