@@ -297,6 +297,86 @@ def bench_c4(dev, iters=30, seed=4, n_slices=64):
     }
 
 
+def bench_c5(dev, iters=20, L=20):
+    """Time-segmented off-resonance SENSE: 256^2, 16 coils, 4 spiral
+    interleaves x 16,384 samples over a 25 ms readout, smooth B0 within
+    +-200 Hz (low-order polynomial + Gaussian bump), L = 20 segments
+    (b0_to_phis_alphas + alpha_segementation, zero-order interpolators as the
+    reference's default); one CG-SENSE solve (20 iterations, lambda 1e-3)
+    and one gradient step on the trajectory through the autograd backward of
+    ||A(k) x - y||^2."""
+    import torch
+    from mr_recon_b200 import synth
+    from mr_recon_b200.field import alpha_segementation, b0_to_phis_alphas
+    from mr_recon_b200.fourier import b200_nufft
+    from mr_recon_b200.linops import sense_linop
+    from mr_recon_b200.recons import CG_SENSE_recon
+    rng = np.random.RandomState(5)
+    N, C, nint, nro = 256, 16, 4, 16384
+    dt = 25e-3 / nro
+    x_np = synth.ellipse_phantom((N, N), 20, rng).astype(np.complex64)
+    mps_np = synth.gaussian_coil_maps((N, N), C).astype(np.complex64)
+    trj_np = synth.vd_spiral(nint, nro, N / 2.0)  # (4, 16384, 2)
+    yy, xx = np.meshgrid(np.linspace(-1, 1, N), np.linspace(-1, 1, N), indexing="ij")
+    b0 = 0.6 * xx + 0.4 * yy - 0.5 * xx * yy + 0.3 * yy ** 2 + np.exp(-((xx - 0.25) ** 2 + (yy + 0.1) ** 2) / 0.08)
+    b0 = (200.0 * b0 / np.abs(b0).max()).astype(np.float32)
+    trj = torch.from_numpy(trj_np).to(dev)
+    mps = torch.from_numpy(mps_np).to(dev)
+    x = torch.from_numpy(x_np).to(dev)
+    t0 = time.perf_counter()
+    phis, alphas = b0_to_phis_alphas(torch.from_numpy(b0).to(dev), (nint, nro), 1, dt)
+    sfun, tfun = alpha_segementation(phis, alphas, L, interp_type="zero", verbose=False)
+    nf = b200_nufft((N, N), oversamp=1.25, width=6)
+    A = sense_linop(trj, mps, nufft=nf, spatial_funcs=sfun, temporal_funcs=tfun)
+    y = A.forward(x)
+    g = torch.Generator(device=dev).manual_seed(5)
+    y = y + torch.randn(y.shape, dtype=torch.complex64, device=dev, generator=g) * (
+        y.abs().square().mean().sqrt() * 10 ** (-30 / 20))
+    v = torch.randn((N, N), dtype=torch.complex64, device=dev, generator=g)
+    for _ in range(15):  # power method for max_eigen (setup)
+        z = A.normal(v)
+        lam = float(torch.linalg.vector_norm(z))
+        v = z / lam
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    rec = CG_SENSE_recon(A, y, max_iter=iters, lamda_l2=1e-3, max_eigen=lam * 1.01, verbose=False)
+    e0, e1 = _events(torch)
+    torch.cuda.synchronize()
+    e0.record()
+    rec = CG_SENSE_recon(A, y, max_iter=iters, lamda_l2=1e-3, max_eigen=lam * 1.01, verbose=False)
+    e1.record()
+    torch.cuda.synchronize()
+    cg_ms = e0.elapsed_time(e1)
+    # CG on A / sqrt(max_eigen) (recons.py:117-123) returns the image scaled by
+    # sqrt(max_eigen): compare after the least-squares complex scale
+    scl = (rec.conj() * x).sum() / (rec.conj() * rec).sum()
+    nrmse = float((scl * rec - x).norm() / x.norm())
+    # one gradient step on the trajectory: loss = ||A(k) x_hat - y||^2
+    k = trj.clone().requires_grad_(True)
+    A2 = sense_linop(k, mps, nufft=nf, spatial_funcs=sfun, temporal_funcs=tfun)
+    xh = (scl * rec).detach()
+    loss = (A2.forward(xh) - y).abs().square().sum()
+    loss.backward()
+    torch.cuda.synchronize()
+    k.grad = None
+    e0.record()
+    loss = (A2.forward(xh) - y).abs().square().sum()
+    loss.backward()
+    with torch.no_grad():
+        k_new = k - 1e-3 * k.grad / (k.grad.abs().max() + 1e-30)
+    e1.record()
+    torch.cuda.synchronize()
+    gs_ms = e0.elapsed_time(e1)
+    return {
+        "workload": "time-segmented B0 SENSE: 256^2, 16 coils, 4x16384 spiral over 25 ms, B0 within "
+                    "+-200 Hz, L=20 segments (zero-order), CG 20 iterations lambda 1e-3",
+        "cg_solve_ms": cg_ms, "solves_per_s": 1e3 / cg_ms, "recon_nrmse_vs_phantom": nrmse,
+        "traj_grad_step_ms": gs_ms, "traj_grad_finite": bool(torch.isfinite(k.grad).all()),
+        "traj_step_max_move": float((k_new - k).abs().max()), "setup_s": setup_s,
+        "coil_segments_per_nufft": C * L,
+    }
+
+
 def run_reference(args, rank):
     """--impl reference: the CPU oracle port of the reference path on the host
     cores, rank 0 only; each step is a bounded sample (a few coils)."""
@@ -331,7 +411,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cg", action="store_true")
-    ap.add_argument("--extra", default="", help="comma list of extra workloads: c3 (3D), c4 (batched CG)")
+    ap.add_argument("--extra", default="", help="comma list of extra workloads: c3 (3D), c4 (batched CG), c5 (B0 segments)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -495,6 +575,8 @@ def main():
             extra["c3"] = bench_c3(dev, 5, peak)
         if "c4" in want:
             extra["c4"] = bench_c4(dev)
+        if "c5" in want:
+            extra["c5"] = bench_c5(dev)
 
     launches_per_step = 4 + (1 if stats["split_tiles"] > 0 else 0)
     if rank == 0:

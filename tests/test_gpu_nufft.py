@@ -444,3 +444,28 @@ def test_sense_cg_graph_matches_oracle():
     x_graph = CG_SENSE_recon(A, T(ksp), max_iter=8, lamda_l2=1e-3, max_eigen=me, verbose=False, graph=True)
     assert rel(Nn(x_eager), ref) < 1e-4
     assert rel(Nn(x_graph), ref) < 1e-4
+
+
+# ----------------------------------------------------------------- time segmentation
+def test_time_segmented_sense_linop_matches_oracle():
+    """sense_linop with B0 spatial / temporal basis functions from
+    alpha_segementation (all coils x segments in one batched NUFFT) against
+    the oracle's segmented SENSE model (linops.py:1134-1228)."""
+    from mr_recon_b200.field import alpha_segementation, b0_to_phis_alphas
+    from mr_recon_b200.linops import sense_linop
+    rng = np.random.RandomState(17)
+    im, C, L = (40, 36), 4, 6
+    trj = synth.vd_spiral(3, 400, 18.0)  # (3, 400, 2)
+    yy, xx = np.meshgrid(np.linspace(-1, 1, im[0]), np.linspace(-1, 1, im[1]), indexing="ij")
+    b0 = (80 * xx - 50 * yy ** 2 + 100 * np.exp(-((xx - 0.2) ** 2 + yy ** 2) / 0.05)).astype(np.float32)
+    phis, alphas = b0_to_phis_alphas(T(b0), (3, 400), 1, 10e-3 / 400)
+    for kind in ("zero", "lstsq"):
+        s, t = alpha_segementation(phis, alphas, L, interp_type=kind, verbose=False)
+        mps = synth.gaussian_coil_maps(im, C).astype(np.complex64)
+        A = sense_linop(T(trj), T(mps), nufft=b200_nufft(im), spatial_funcs=s, temporal_funcs=t)
+        on = O.KBNufftOracle(im, 1.25, 6)
+        Ao = O.SenseOracle(trj, mps, on, spatial_funcs=Nn(s), temporal_funcs=Nn(t))
+        x = synth.randn_complex(im, rng)
+        y = synth.randn_complex((C, 3, 400), rng)
+        assert rel(Nn(A.forward(T(x))), Ao.forward(x)) < TOL
+        assert rel(Nn(A.adjoint(T(y))), Ao.adjoint(y)) < TOL
