@@ -140,7 +140,7 @@ def _events(torch):
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
 
-def bench_c3(dev, steps, peak):
+def bench_c3(dev, steps, peak, N=192, spokes=20000):
     """3D NUFFT with autograd: 192^3, 16 coils, kooshball 20,000 x 384,
     os 1.25, W 4. fwd+adj Msample*coil/s with the gridding roofline (the
     path's HBM-bound case), and one loss / backward step with image and
@@ -148,8 +148,8 @@ def bench_c3(dev, steps, peak):
     import torch
     from mr_recon_b200.fourier import b200_nufft
     from mr_recon_b200 import synth
-    N, C = 192, 16
-    trj = torch.from_numpy(synth.kooshball(20000, 384, N / 2.0).reshape(1, -1, 3)).to(dev)
+    C = 16
+    trj = torch.from_numpy(synth.kooshball(spokes, 2 * N, N / 2.0).reshape(1, -1, 3)).to(dev)
     M = trj.shape[1]
     g = torch.Generator(device=dev).manual_seed(3)
     img = torch.randn((1, C, N, N, N), dtype=torch.complex64, device=dev, generator=g)
@@ -193,7 +193,7 @@ def bench_c3(dev, steps, peak):
     ag_ms = e0.elapsed_time(e1)
     stats = plan.stats()
     return {
-        "workload": "3D KB NUFFT fwd+adj: 192^3 c64, 16 coils, kooshball 20000x384, os 1.25, W 4",
+        "workload": f"3D KB NUFFT fwd+adj: {N}^3 c64, 16 coils, kooshball {spokes}x{2 * N}, os 1.25, W 4",
         "value": C * M / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": ms, "steps": steps,
         "stage_ms": {k2: v[0] / steps for k2, v in st.items() if v[1]},
         "grid_roofline": {"bound": "hbm", "algorithmic_bytes": alg, "kernel_ms": g_ms,
@@ -411,6 +411,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cg", action="store_true")
+    ap.add_argument("--c3-n", type=int, default=192, help="c3 image edge (192 = the configuration)")
+    ap.add_argument("--c3-spokes", type=int, default=20000, help="c3 kooshball spokes (20000 = the configuration)")
     ap.add_argument("--extra", default="", help="comma list of extra workloads: c3 (3D), c4 (batched CG), c5 (B0 segments)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -572,7 +574,7 @@ def main():
     if rank == 0 and world == 1:
         want = [e.strip() for e in args.extra.split(",") if e.strip()]
         if "c3" in want:
-            extra["c3"] = bench_c3(dev, 5, peak)
+            extra["c3"] = bench_c3(dev, 5, peak, args.c3_n, args.c3_spokes)
         if "c4" in want:
             extra["c4"] = bench_c4(dev)
         if "c5" in want:

@@ -73,6 +73,7 @@ k_pre(const SliceGeom* __restrict__ sl, int ns, const float* __restrict__ apod,
     srow = src + g.img_off + (int64_t)c * g.nimg + qlin;
   }
   const int h = nl / 2;
+#pragma unroll 4
   for (int j = lane; j < nosl; j += 32) {
     int q = j + h;
     if (q >= nosl) q -= nosl;
@@ -131,6 +132,7 @@ k_post(const SliceGeom* __restrict__ sl, int ns, const float* __restrict__ apod,
   if (mode == kPostPlain) {
     const float2* yrow = grid + g.grid_off + (int64_t)c_plain * g.gos + slin;
     float2* orow_p = out + g.img_off + (int64_t)c_plain * g.nimg + orow * nl;
+#pragma unroll 4
     for (int j = lane; j < nl; j += 32) {
       int sj = j - h;
       if (sj < 0) sj += nosl;
@@ -145,6 +147,7 @@ k_post(const SliceGeom* __restrict__ sl, int ns, const float* __restrict__ apod,
       int sj = j - h;
       if (sj < 0) sj += nosl;
       float ax = 0.f, ay = 0.f;
+#pragma unroll 4
       for (int c = 0; c < g.ncoil; ++c) {
         const float2 y = grid[g.grid_off + (int64_t)c * g.gos + slin + sj];
         const float2 m = __ldg(mps + g.img_off + (int64_t)c * g.nimg + orow * nl + j);

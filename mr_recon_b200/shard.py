@@ -2,9 +2,9 @@
 
 The NUFFT / CG-SENSE path shards by problem: slices of an uneven batch (and
 replicas of a problem) are independent, so ranks exchange nothing on the
-data path (SURVEY config 4; the reference has no multi-GPU path). What ranks
-do share is bookkeeping: which slices each rank solves, and the job time,
-which is the maximum of the ranks' device times.
+data path (the reference has no multi-GPU path). What ranks do share is
+bookkeeping: which slices each rank solves, and the job time, which is the
+maximum of the ranks' device times.
 """
 
 from __future__ import annotations
