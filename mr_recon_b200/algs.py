@@ -22,7 +22,8 @@ from tqdm import tqdm
 
 complex_dtype = torch.complex64
 
-__all__ = ["conjugate_gradient", "power_method_operator", "FISTA", "gradient_descent", "SenseCG"]
+__all__ = ["conjugate_gradient", "power_method_operator", "FISTA", "gradient_descent", "SenseCG",
+           "density_compensation"]
 
 
 def _rdot(a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
@@ -217,3 +218,46 @@ class SenseCG:
 
     def iterations(self) -> torch.Tensor:
         return self.state.view(-1, 8)[:, 5]
+
+
+def density_compensation(trj: torch.Tensor, im_size: tuple, num_iters: Optional[int] = 30,
+                         method: str = "sigpy", width: float = 4.0, beta: float = 8.0) -> torch.Tensor:
+    """Pipe-Menon density compensation (algs.py:20-106), normalised to max 1.
+
+    The reference delegates to sigpy.mri.pipe_menon_dcf (sigpy is not pinned in
+    its environment.yml and not present here). This restates the published
+    iteration (Pipe & Menon, MRM 41:179-186, 1999) on the B200 gridding and
+    interpolation kernels: with G the Kaiser-Bessel gridding operator from the
+    samples onto the image-size grid (width 4, beta 8, no oversampling, as the
+    sigpy routine), w <- w / |G^H G w| for ``num_iters`` iterations, starting
+    from w = 1; G^H G w then approaches 1 on every sample. The kernel's overall
+    scale cancels in the final normalisation.
+
+    trj : (..., d) in grid units, k_i in [-N_i/2, N_i/2) (CUDA tensor)
+    returns (...) float32
+    """
+    from . import _lib
+    from .plan import Plan
+    if method.lower() != "sigpy":
+        raise NotImplementedError("only the Pipe-Menon iteration ('sigpy') is provided")
+    _lib.require_cuda(trj, "trajectory")
+    d = trj.shape[-1]
+    im_size = tuple(int(n) for n in im_size)
+    if len(im_size) != d:
+        raise ValueError(f"trajectory has {d} dims, im_size {len(im_size)}")
+    tshape = trj.shape[:-1]
+    locs = trj.detach().to(torch.float32).reshape(-1, d)
+    locs = locs + torch.tensor([n // 2 for n in im_size], dtype=torch.float32, device=trj.device)
+    M = locs.shape[0]
+    plan = Plan([im_size], [M], [1], 1.0, (float(width),) * d, float(beta), raw=True, device=trj.device)
+    plan.set_traj(locs.contiguous().reshape(-1))
+    w = torch.ones(M, dtype=torch.complex64, device=trj.device)
+    g = torch.empty(plan.n_grid, dtype=torch.complex64, device=trj.device)
+    ghgw = torch.empty_like(w)
+    for _ in range(int(num_iters)):
+        plan.grid(w, g, 1.0)
+        plan.interp(g, ghgw, 1.0)
+        w = w / ghgw.abs()
+    dcf = w.real.reshape(tshape)
+    return dcf / dcf.max()
+

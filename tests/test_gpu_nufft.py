@@ -469,3 +469,31 @@ def test_time_segmented_sense_linop_matches_oracle():
         y = synth.randn_complex((C, 3, 400), rng)
         assert rel(Nn(A.forward(T(x))), Ao.forward(x)) < TOL
         assert rel(Nn(A.adjoint(T(y))), Ao.adjoint(y)) < TOL
+
+
+# ----------------------------------------------------------------- density compensation
+def test_density_compensation_pipe_menon_properties():
+    """Pipe-Menon DCF on the B200 kernels (the reference calls sigpy, absent
+    here, so parity is pinned by the defining property): after the
+    iterations G^H G w is flat over the samples, and for a radial trajectory
+    the weights grow with |k| (the ramp), with a denser centre getting less
+    weight."""
+    from mr_recon_b200.algs import density_compensation
+    from mr_recon_b200.interp import grid as mgrid, ungrid as mungrid
+    im = (64, 64)
+    trj = synth.golden_angle_radial(96, 128, 32.0)  # (96, 128, 2)
+    t = T(trj)
+    dcf = density_compensation(t, im, num_iters=30)
+    assert dcf.shape == trj.shape[:-1] and float(dcf.max()) == pytest.approx(1.0)
+    locs = (t + 32.0).reshape(-1, 2)
+    w = dcf.reshape(-1).to(torch.complex64)
+    kp = {"beta": 8.0}
+    ghgw = mungrid(mgrid(w, locs, im, (4, 4), kernel_params=kp), locs, (4, 4), kernel_params=kp).abs()
+    flat = ghgw / ghgw.mean()
+    assert float((flat - 1).abs().quantile(0.9)) < 0.05
+    r = torch.linalg.vector_norm(t, dim=-1).reshape(-1)
+    d = dcf.reshape(-1)
+    inner = d[(r > 2) & (r < 8)].mean()
+    mid = d[(r > 14) & (r < 20)].mean()
+    outer = d[(r > 24) & (r < 30)].mean()
+    assert float(inner) < float(mid) < float(outer)
