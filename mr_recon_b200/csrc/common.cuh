@@ -101,6 +101,23 @@ __device__ __forceinline__ float kb_tap_series(float adx, float inv_r, const KBP
   return w;
 }
 
+// Weight and its derivative along the sample coordinate u for a tap at
+// dx = j - u: with p(t) the series above, t = 1 - x^2, x = |dx| / r,
+// dw/du = p'(t) * (dt/dx) * (dx/du) = p'(t) * (-2x) * (-sign(dx)) / r.
+// p and p' come from one Horner pass (the derivative recurrence d <- d t + p).
+__device__ __forceinline__ float2 kb_tap_series_du(float dx, float inv_r, const KBParams& kb) {
+  const float x = fabsf(dx) * inv_r;
+  const float t = fmaxf(1.0f - x * x, 0.0f);
+  float p = kb.coef[kKBTerms - 1], d = 0.0f;
+#pragma unroll
+  for (int k = kKBTerms - 2; k >= 0; --k) {
+    d = fmaf(d, t, p);
+    p = fmaf(p, t, kb.coef[k]);
+  }
+  const float sgn = dx > 0.0f ? 1.0f : (dx < 0.0f ? -1.0f : 0.0f);
+  return make_float2(p, d * 2.0f * x * sgn * inv_r);
+}
+
 // Weight used by the fast tile kernels: the series when it converges within
 // kKBTerms terms for this beta (every beta reachable with W < 8), else A&S.
 __device__ __forceinline__ float kb_tap_fast(float adx, float inv_r, const KBParams& kb) {

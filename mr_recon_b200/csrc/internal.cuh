@@ -31,6 +31,8 @@ int launch_grid_warp(mrn_plan* P, const float2* ksp, const float* dcf, const flo
 bool interp_reg_ok(const mrn_plan* P);
 int launch_interp_reg(mrn_plan* P, const float2* grid, int layout, float2* ksp, float scale,
                       const float2* temporal, cudaStream_t st);
+int launch_trajgrad_reg(mrn_plan* P, const float2* grid, int layout, const float2* samples, float* out,
+                        float scale, cudaStream_t st);
 bool grid_reg_ok(const mrn_plan* P);
 bool grid_reg3_ok(const mrn_plan* P);
 int launch_grid_reg3(mrn_plan* P, const float2* ksp, const float* dcf, const float2* temporal,

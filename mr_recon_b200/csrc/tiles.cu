@@ -824,6 +824,8 @@ int launch_traj_grad(mrn_plan* P, const float2* grid, GridLayout layout, const f
   cudaError_t e = cudaMemsetAsync(out, 0, (size_t)P->n_trj * sizeof(float), st);
   if (e != cudaSuccess) return cuda_fail(e);
   if (P->n_items_interp == 0) return MRN_OK;
+  if (P->use_fast && fast_path_ok(P, false) && interp_reg_ok(P))
+    return launch_trajgrad_reg(P, grid, (int)layout, samples, out, scale, st);
   const Layout L = plan_layout(P, 2);
   const int G = pick_g(L.cg);
   dim3 gridDim((unsigned)P->n_items_interp, (unsigned)((P->max_coil + L.cg - 1) / L.cg));

@@ -575,6 +575,46 @@ k_grid_warp(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
 // (fma.rn.f32x2: real and imaginary part in one instruction), one shared
 // load per tap, then combines the rows with the outer weights.
 // ---------------------------------------------------------------------------
+// Region load of the lane-per-coil kernels: the tile region (ext cells,
+// wrapped) of ncg coil planes into shared memory as [cell][coil] with coil
+// stride CS. Thread = one cell, looping over the coil planes with the global
+// address stepped by the plane stride; kLoadBatch loads in flight per thread.
+// Consecutive threads read consecutive cells of a row and write shared words
+// 2 * CS apart (CS odd: no bank conflict).
+template <int D, int CS>
+__device__ __forceinline__ void load_region_cc(float2* __restrict__ region, const float2* __restrict__ gbase,
+                                               int64_t gos, int ncg, const Frame& f, const int* ext,
+                                               const int* nos, const int* hs, int tid, int nthreads) {
+  constexpr int kLoadBatch = 8;
+  const int inner = ext[D - 1];
+  const int ncells = ext[0] * ext[1] * ext[2];
+  for (int cell = tid; cell < ncells; cell += nthreads) {
+    int64_t off;
+    if (D == 2) {
+      const int r = cell / inner, q = cell - r * inner;
+      off = (int64_t)wrap_cells(f.org[0] + r - hs[0], nos[0]) * nos[1] +
+            wrap_cells(f.org[1] + q - hs[1], nos[1]);
+    } else {
+      const int rz = cell / inner, z = cell - rz * inner;
+      const int x = rz / ext[1], y = rz - x * ext[1];
+      off = ((int64_t)wrap_cells(f.org[0] + x - hs[0], nos[0]) * nos[1] +
+             wrap_cells(f.org[1] + y - hs[1], nos[1])) * nos[2] +
+            wrap_cells(f.org[2] + z - hs[2], nos[2]);
+    }
+    const float2* src = gbase + off;
+    float2* dst = region + cell * CS;
+    for (int cb = 0; cb < ncg; cb += kLoadBatch) {
+      float2 v[kLoadBatch];
+#pragma unroll
+      for (int u = 0; u < kLoadBatch; ++u)
+        if (cb + u < ncg) v[u] = __ldg(src + (int64_t)(cb + u) * gos);
+#pragma unroll
+      for (int u = 0; u < kLoadBatch; ++u)
+        if (cb + u < ncg) dst[cb + u] = v[u];
+    }
+  }
+}
+
 constexpr int kRegInterpWarps = 8;
 constexpr int kInterpStage = 128;  // samples whose coordinates are staged at once
 
@@ -620,39 +660,7 @@ k_interp_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, K
       s_u[j] = coord[it.start + sb + j];
       s_p[j] = (int)(perm[it.start + sb + j] - pt_off);
     }
-    if (sb == 0) {
-      // region: thread = one cell, looping over the coil planes with the
-      // global address stepped by the plane stride; kLoadBatch loads in
-      // flight per thread. Consecutive threads read consecutive cells of a
-      // row and write shared words 2 * CS apart (CS odd: no bank conflict).
-      constexpr int kLoadBatch = 8;
-      const int ncells = ext[0] * ext[1] * ext[2];
-      for (int cell = tid; cell < ncells; cell += NT) {
-        int64_t off;
-        if (D == 2) {
-          const int r = cell / inner, q = cell - r * inner;
-          off = (int64_t)wrap_cells(f.org[0] + r - hs[0], nos[0]) * nos[1] +
-                wrap_cells(f.org[1] + q - hs[1], nos[1]);
-        } else {
-          const int rz = cell / inner, z = cell - rz * inner;
-          const int x = rz / ext[1], y = rz - x * ext[1];
-          off = ((int64_t)wrap_cells(f.org[0] + x - hs[0], nos[0]) * nos[1] +
-                 wrap_cells(f.org[1] + y - hs[1], nos[1])) * nos[2] +
-                wrap_cells(f.org[2] + z - hs[2], nos[2]);
-        }
-        const float2* src = gbase + off;
-        float2* dst = region + cell * CS;
-        for (int cb = 0; cb < ncg; cb += kLoadBatch) {
-          float2 v[kLoadBatch];
-#pragma unroll
-          for (int u = 0; u < kLoadBatch; ++u)
-            if (cb + u < ncg) v[u] = __ldg(src + (int64_t)(cb + u) * gos);
-#pragma unroll
-          for (int u = 0; u < kLoadBatch; ++u)
-            if (cb + u < ncg) dst[cb + u] = v[u];
-        }
-      }
-    }
+    if (sb == 0) load_region_cc<D, CS>(region, gbase, gos, ncg, f, ext, nos, hs, tid, NT);
     __syncthreads();
 
     for (int base = warp * SUB; base < ns; base += NW * SUB) {
@@ -713,6 +721,166 @@ k_interp_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, K
         *dst = make_float2(o.x + v.x, o.y + v.y);
       } else {
         *dst = v;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Trajectory gradient, lane = coil: d/du_i Re sum_c conj(S_c) (A x)_c at each
+// sample, the same region staging and sample loop as k_interp_reg. Per
+// sample each lane forms, for its coil, the separable sums with one factor
+// replaced by the weight's derivative (2D: row sums with w1 and dw1, then
+// dw0 / w0; 3D: row sums with w2 and dw2, plane sums with w1 / dw1, then
+// dw0 / w0), takes Re(conj(S_c) .) and the sample's lanes sum over their
+// coils with shuffles; one atomic add per sample and dimension (coil groups
+// of one slice add into the same output).
+// ---------------------------------------------------------------------------
+template <int D, int K, int SUB>
+__global__ void __launch_bounds__(kRegInterpWarps * 32)
+k_trajgrad_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBParams kb,
+               const float4* __restrict__ coord, const int* __restrict__ perm,
+               const float2* __restrict__ grid, int layout, const float2* __restrict__ samp,
+               float* __restrict__ out, float scale, int cg) {
+  constexpr int CW = 32 / SUB, CS = CW + 1, NW = kRegInterpWarps, NT = NW * 32;
+  extern __shared__ float4 smem_f4[];
+  float2* region = reinterpret_cast<float2*>(smem_f4);
+  __shared__ float4 s_u[kInterpStage];
+  __shared__ int s_p[kInterpStage];
+
+  const Item it = items[blockIdx.x];
+  const SliceGeom* gp = sl + it.slice;
+  const int ncoil = gp->ncoil;
+  const int c0 = blockIdx.y * cg;
+  if (c0 >= ncoil) return;
+  const int ncg = min(cg, ncoil - c0);
+  int nos[3], hs[3], ext[3];
+  const Frame f = frame_of(*gp, it.tile, D, false);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    nos[i] = gp->nos[i];
+    hs[i] = (i < D && layout == kInternal) ? gp->hshift[i] : 0;
+    ext[i] = i < D ? f.size[i] + K - 1 : 1;
+  }
+  const int inner = ext[D - 1];
+  const int64_t gos = gp->gos;
+  const float2* gbase = grid + (layout == kInternal ? gp->grid_off : gp->ugrid_off) + (int64_t)c0 * gos;
+  const int64_t m = gp->m, pt_off = gp->pt_off;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int coil = lane % CW, sub = lane / CW;
+  const bool has_coil = coil < ncg;
+  const float2* sampc = samp + gp->ksp_off + (int64_t)(c0 + (has_coil ? coil : 0)) * m;
+  const float osc[3] = {scale * gp->scale[0], scale * gp->scale[1], scale * gp->scale[2]};
+
+  for (int sb = 0; sb < it.count; sb += kInterpStage) {
+    const int ns = min(kInterpStage, it.count - sb);
+    if (sb > 0) __syncthreads();
+    for (int j = tid; j < ns; j += NT) {
+      s_u[j] = coord[it.start + sb + j];
+      s_p[j] = perm[it.start + sb + j];
+    }
+    if (sb == 0) load_region_cc<D, CS>(region, gbase, gos, ncg, f, ext, nos, hs, tid, NT);
+    __syncthreads();
+
+    for (int base = warp * SUB; base < ns; base += NW * SUB) {
+      const int el = base + sub;
+      const bool active = el < ns;
+      const float4 uu = s_u[active ? el : base];
+      const int pm = s_p[active ? el : base];
+      const float2 sv = (active && has_coil) ? __ldg(sampc + (pm - pt_off)) : make_float2(0.f, 0.f);
+      const float u[3] = {uu.x, uu.y, uu.z};
+      int lo[3] = {0, 0, 0}, l0[3] = {0, 0, 0};
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        lo[i] = (int)ceilf(__fsub_rn(u[i], kb.radius[i]));
+        l0[i] = wrap_once(lo[i], nos[i]) - f.org[i];
+      }
+      // weight and derivative of tap t = i*K + q, computed by the sample's lanes, broadcast
+      constexpr int NWT = D * K, IT = (NWT + CW - 1) / CW;
+      const int lg = lane % CW, lbase = lane - lg;
+      float2 mine[IT];
+#pragma unroll
+      for (int k2 = 0; k2 < IT; ++k2) {
+        const int t = k2 * CW + lg;
+        float2 v = make_float2(0.f, 0.f);
+        if (t < NWT) {
+          const int i = t / K, q = t - (t / K) * K;
+          const float ui = sel3(u, i), ri = sel3(kb.radius, i);
+          const float dx = __fsub_rn((float)(sel3(lo, i) + q), ui);
+          if (fabsf(dx) <= ri) {
+            if (kb.series) {
+              v = kb_tap_series_du(dx, sel3(kb.inv_radius, i), kb);
+            } else {
+              v = make_float2(kb_tap(fabsf(dx), ri, kb.beta), kb_tap_du(dx, ri, kb.beta));
+            }
+          }
+        }
+        mine[k2] = v;
+      }
+      float w[D][K], dw[D][K];
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+          const int t = i * K + q;
+          w[i][q] = __shfl_sync(0xffffffffu, mine[t / CW].x, lbase + (t % CW));
+          dw[i][q] = __shfl_sync(0xffffffffu, mine[t / CW].y, lbase + (t % CW));
+        }
+      float g[3] = {0.f, 0.f, 0.f};
+      if (active && has_coil) {
+        float2 a0 = make_float2(0.f, 0.f), a1 = a0, a2 = a0;
+        if (D == 2) {
+          const float2* rb = region + (l0[0] * inner + l0[1]) * CS + coil;
+#pragma unroll
+          for (int a = 0; a < K; ++a) {
+            const float2* rp = rb + a * inner * CS;
+            float2 r = make_float2(0.f, 0.f), rd = r;
+#pragma unroll
+            for (int b = 0; b < K; ++b) {
+              const float2 gv = rp[b * CS];
+              r = __ffma2_rn(make_float2(w[1][b], w[1][b]), gv, r);
+              rd = __ffma2_rn(make_float2(dw[1][b], dw[1][b]), gv, rd);
+            }
+            a0 = __ffma2_rn(make_float2(dw[0][a], dw[0][a]), r, a0);
+            a1 = __ffma2_rn(make_float2(w[0][a], w[0][a]), rd, a1);
+          }
+        } else {
+          const float2* rb = region + ((l0[0] * ext[1] + l0[1]) * inner + l0[D - 1]) * CS + coil;
+#pragma unroll
+          for (int a = 0; a < K; ++a) {
+            float2 p = make_float2(0.f, 0.f), p1 = p, p2 = p;
+#pragma unroll
+            for (int b = 0; b < K; ++b) {
+              const float2* rp = rb + (a * ext[1] + b) * inner * CS;
+              float2 r = make_float2(0.f, 0.f), rd = r;
+#pragma unroll
+              for (int c = 0; c < K; ++c) {
+                const float2 gv = rp[c * CS];
+                r = __ffma2_rn(make_float2(w[D - 1][c], w[D - 1][c]), gv, r);
+                rd = __ffma2_rn(make_float2(dw[D - 1][c], dw[D - 1][c]), gv, rd);
+              }
+              p = __ffma2_rn(make_float2(w[1][b], w[1][b]), r, p);
+              p1 = __ffma2_rn(make_float2(dw[1][b], dw[1][b]), r, p1);
+              p2 = __ffma2_rn(make_float2(w[1][b], w[1][b]), rd, p2);
+            }
+            a0 = __ffma2_rn(make_float2(dw[0][a], dw[0][a]), p, a0);
+            a1 = __ffma2_rn(make_float2(w[0][a], w[0][a]), p1, a1);
+            a2 = __ffma2_rn(make_float2(w[0][a], w[0][a]), p2, a2);
+          }
+        }
+        // Re(conj(S) * acc)
+        g[0] = sv.x * a0.x + sv.y * a0.y;
+        g[1] = sv.x * a1.x + sv.y * a1.y;
+        g[2] = sv.x * a2.x + sv.y * a2.y;
+      }
+      // sum over the sample's coil lanes
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int o = CW / 2; o > 0; o >>= 1) g[i] += __shfl_xor_sync(0xffffffffu, g[i], o);
+      if (active && coil == 0) {
+#pragma unroll
+        for (int i = 0; i < D; ++i) atomicAdd(out + (int64_t)pm * D + i, g[i] * osc[i]);
       }
     }
   }
@@ -1279,6 +1447,42 @@ int launch_interp_reg(mrn_plan* P, const float2* grid, int layout, float2* ksp, 
 #undef MRN_IREG_K
 #undef MRN_IREG_SUB
 #undef MRN_IREG_LAUNCH
+  if (rc != MRN_OK) return rc;
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? MRN_OK : cuda_fail(e);
+}
+
+int launch_trajgrad_reg(mrn_plan* P, const float2* grid, int layout, const float2* samples, float* out,
+                        float scale, cudaStream_t st) {
+  if (P->n_items_interp == 0) return MRN_OK;
+  int cg, ng;
+  const int sub = interp_reg_sub(P, &cg, &ng);
+  const size_t smem = interp_reg_smem(P, sub);
+  const dim3 gdim((unsigned)P->n_items_interp, (unsigned)ng);
+  const int K = P->kb.ntaps[0];
+  int rc = MRN_OK;
+#define MRN_TG_LAUNCH(DD, KK, SS)                                                                   \
+  do {                                                                                              \
+    auto kern = k_trajgrad_reg<DD, KK, SS>;                                                         \
+    rc = prep_attr(kern, smem);                                                                     \
+    if (rc == MRN_OK)                                                                               \
+      kern<<<gdim, kRegInterpWarps * 32, smem, st>>>(P->d_items_i, P->d_slices, P->kb, P->d_coord_i, \
+                                                     P->d_perm_i, grid, layout, samples, out, scale, cg); \
+  } while (0)
+#define MRN_TG_SUB(DD, KK)                     \
+  if (sub == 4) MRN_TG_LAUNCH(DD, KK, 4);      \
+  else if (sub == 2) MRN_TG_LAUNCH(DD, KK, 2); \
+  else MRN_TG_LAUNCH(DD, KK, 1)
+#define MRN_TG_K(DD)                      \
+  if (K == 5) { MRN_TG_SUB(DD, 5); }      \
+  else if (K == 6) { MRN_TG_SUB(DD, 6); } \
+  else if (K == 7) { MRN_TG_SUB(DD, 7); } \
+  else { MRN_TG_SUB(DD, 8); }
+  if (P->ndim == 2) { MRN_TG_K(2) }
+  else { MRN_TG_K(3) }
+#undef MRN_TG_K
+#undef MRN_TG_SUB
+#undef MRN_TG_LAUNCH
   if (rc != MRN_OK) return rc;
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? MRN_OK : cuda_fail(e);
