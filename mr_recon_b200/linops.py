@@ -116,6 +116,16 @@ class sense_linop(linop):
             else:
                 self.plan.set_traj(trj.contiguous())
 
+        # zero-order time segments (alpha_segementation's default): every sample
+        # lies in exactly one segment, so A = sum_l P_l A_l B_l with disjoint
+        # sample selections P_l and A^H A = sum_l conj(b_l) A_l^H A_l (b_l x):
+        # one uneven multi-slice plan, slice l = segment l's samples, runs the
+        # whole operator with each sample interpolated / gridded once
+        self.seg = None
+        if (isinstance(nufft, b200_nufft) and self.segmented and not use_toeplitz
+                and not trj.requires_grad):
+            self.seg = self._segment_plan(nufft, trj, mps, dcf, spatial_funcs, temporal_funcs)
+
         if use_toeplitz:
             # linops.py:1102-1119: the spatial/temporal defaults are already in
             # place here, so the reference always builds (L, L, *im_os) kernels
@@ -132,8 +142,55 @@ class sense_linop(linop):
             self.toep_kerns = None
 
     # ------------------------------------------------------------------
+    def _segment_plan(self, nufft, trj, mps, dcf, spatial, temporal):
+        """Multi-slice plan of a one-hot (zero-order) segmentation, or None
+        when the temporal functions are not one-hot or the shapes differ."""
+        L = temporal.shape[0]
+        im, ts = self.im_size, self.trj_size
+        if spatial.shape[0] != L or tuple(spatial.shape[1:]) != tuple(im):
+            return None
+        tf = temporal.expand((L, *ts))
+        nz = tf != 0
+        if not bool((nz.sum(0) == 1).all()) or not bool((tf[nz] == 1).all()):
+            return None
+        dev = trj.device
+        M = int(nz[0].numel())
+        d = trj.shape[-1]
+        C = mps.shape[0]
+        inds = nz.reshape(L, M).to(torch.int32).argmax(0)
+        order = torch.argsort(inds, stable=True)
+        counts = torch.bincount(inds, minlength=L)
+        plan = Plan([tuple(im)] * L, [int(c) for c in counts.tolist()], [C] * L, nufft.oversamp,
+                    nufft._widths(), nufft.beta, apodize=nufft.apodize, tile=nufft.tile,
+                    coil_group=nufft.coil_group, max_chunk=nufft.max_chunk, device=dev,
+                    fast=nufft.fast, warp_grid=nufft.warp_grid, weight_tables=nufft.weight_tables,
+                    reg_grid=nufft.reg_grid, reg_interp=nufft.reg_interp)
+        plan.set_traj(trj.reshape(M, d)[order].contiguous().reshape(-1))
+        # plan k-space position of (coil c, sample t): ksp_off[l] + c * M_l + rank of t in l
+        start = torch.cumsum(counts, 0) - counts
+        pos = torch.empty(M, dtype=torch.int64, device=dev)
+        pos[order] = torch.arange(M, device=dev)
+        koff = torch.as_tensor(plan.ksp_off, dtype=torch.int64, device=dev)
+        base = koff[inds] + (pos - start[inds])
+        src = (base[None, :] + torch.arange(C, device=dev)[:, None] * counts[inds][None, :]).reshape(-1)
+        return {"plan": plan, "src": src, "L": L,
+                "mps": mps.reshape(1, -1).expand(L, -1).contiguous().reshape(-1),
+                "dcf": dcf.reshape(M)[order].contiguous(),
+                "b": spatial.to(complex_dtype).reshape(L, -1).contiguous()}
+
+    def _use_seg(self, *tensors):
+        if self.seg is None:
+            return False
+        return not (torch.is_grad_enabled() and any(t.requires_grad for t in tensors))
+
     def forward(self, img: torch.Tensor) -> torch.Tensor:
         """(*im_size) -> (C, *trj_size)."""
+        if self._use_seg(img):
+            sg = self.seg
+            xl = (sg["b"] * img.to(complex_dtype).reshape(1, -1)).reshape(-1)
+            kp = torch.empty(sg["plan"].n_ksp, dtype=complex_dtype, device=img.device)
+            sg["plan"].sense_forward(xl, sg["mps"], kp)
+            return kp[sg["src"]].reshape((self.mps.shape[0], *self.trj_size))
         if self.plan is not None:
             x = img.to(complex_dtype).contiguous()
             ksp = torch.empty((self.mps.shape[0], *self.trj_size), dtype=complex_dtype, device=x.device)
@@ -151,6 +208,13 @@ class sense_linop(linop):
 
     def adjoint(self, ksp: torch.Tensor) -> torch.Tensor:
         """(C, *trj_size) -> (*im_size)."""
+        if self._use_seg(ksp):
+            sg = self.seg
+            kp = torch.empty(sg["plan"].n_ksp, dtype=complex_dtype, device=ksp.device)
+            kp[sg["src"]] = ksp.to(complex_dtype).reshape(-1)
+            xl = torch.empty_like(sg["b"])
+            sg["plan"].sense_adjoint(kp, sg["dcf"], sg["mps"], xl)
+            return (sg["b"].conj() * xl).sum(0).reshape(self.im_size)
         if self.plan is not None:
             y = ksp.to(complex_dtype).contiguous()
             img = torch.empty(self.im_size, dtype=complex_dtype, device=y.device)
@@ -169,6 +233,12 @@ class sense_linop(linop):
     def normal(self, img: torch.Tensor) -> torch.Tensor:
         """A^H A x (linops.py:1230-1308)."""
         if not self.use_toeplitz:
+            if self._use_seg(img):
+                sg = self.seg
+                xl = (sg["b"] * img.to(complex_dtype).reshape(1, -1)).contiguous()
+                out = torch.empty_like(xl)
+                sg["plan"].sense_normal(xl, sg["mps"], sg["dcf"], out)
+                return (sg["b"].conj() * out).sum(0).reshape(self.im_size)
             if self.plan is not None:
                 x = img.to(complex_dtype).contiguous()
                 out = torch.empty_like(x)

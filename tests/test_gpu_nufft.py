@@ -467,8 +467,10 @@ def test_time_segmented_sense_linop_matches_oracle():
         Ao = O.SenseOracle(trj, mps, on, spatial_funcs=Nn(s), temporal_funcs=Nn(t))
         x = synth.randn_complex(im, rng)
         y = synth.randn_complex((C, 3, 400), rng)
+        assert (A.seg is not None) == (kind == "zero")  # one-hot segments use the multi-slice plan
         assert rel(Nn(A.forward(T(x))), Ao.forward(x)) < TOL
         assert rel(Nn(A.adjoint(T(y))), Ao.adjoint(y)) < TOL
+        assert rel(Nn(A.normal(T(x))), Ao.adjoint(Ao.forward(x))) < TOL
 
 
 # ----------------------------------------------------------------- density compensation
