@@ -473,10 +473,13 @@ def main():
     plan.enable_timing(True)
     plan.timing()  # clear
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    host_s = 0.0
     for i in range(args.steps):
         flush.zero_()
         evs[i][0].record()
+        h0 = time.perf_counter()
         step()
+        host_s += time.perf_counter() - h0
         evs[i][1].record()
     torch.cuda.synchronize()
     if world > 1:
@@ -499,7 +502,8 @@ def main():
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                 "algorithmic_bytes": alg, "kernel_ms": dms,
-                "stage_ms_per_step": {k: v[0] / args.steps for k, v in stage.items() if v[1]}}
+                "stage_ms_per_step": {k: v[0] / args.steps for k, v in stage.items() if v[1]},
+                "host_enqueue_ms_per_step": host_s * 1e3 / args.steps}
 
     # end to end through the public API with pinned host buffers
     img_h = imgs.cpu().pin_memory()

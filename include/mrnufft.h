@@ -101,8 +101,9 @@ int mrn_plan_stats(mrn_plan* plan, int64_t* out4);
 /* Work decomposition (each takes effect at the next mrn_plan_set_traj):
  * MRN_OPT_INTERP_CHUNK / MRN_OPT_GRID_CHUNK: samples per interpolation work
  * item and gridding entries per gridding work item (defaults: 256 / 256 in
- * 2D, 1024 otherwise); MRN_OPT_INTERP_TILE / MRN_OPT_GRID_TILE: tile edge in
- * grid cells, every dimension (defaults: 10 / 8 in 2D, 6 / 8 in 3D, 256 in 1D). */
+ * 2D, 1024 / 4096 in 3D, 1024 in 1D); MRN_OPT_INTERP_TILE / MRN_OPT_GRID_TILE:
+ * tile edge in grid cells, every dimension (defaults: 10 / 8 in 2D, 4 / 8 in
+ * 3D, 256 in 1D). */
 #define MRN_OPT_INTERP_CHUNK 4
 #define MRN_OPT_GRID_CHUNK 5
 #define MRN_OPT_INTERP_TILE 6

@@ -39,8 +39,8 @@ def default_candidates(ndim: int) -> dict:
         return {"interp_tile": [8, 10, 12], "interp_chunk": [128, 256],
                 "grid_tile": [6, 8], "grid_chunk": [128, 192, 256, 384]}
     if ndim == 3:
-        return {"interp_tile": [6, 8], "interp_chunk": [256, 1024],
-                "grid_tile": [6, 8], "grid_chunk": [512, 1024, 2048]}
+        return {"interp_tile": [4, 5, 6], "interp_chunk": [256, 1024],
+                "grid_tile": [6, 8], "grid_chunk": [1024, 2048, 4096]}
     return {"interp_tile": [128, 256], "interp_chunk": [512, 1024],
             "grid_tile": [128, 256], "grid_chunk": [512, 1024]}
 

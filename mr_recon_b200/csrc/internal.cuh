@@ -8,6 +8,16 @@ namespace mrn {
 int cuda_fail(cudaError_t e);
 extern thread_local int g_last_cuda_error;
 
+// Opt a kernel into `dyn` bytes of dynamic shared memory when its static plus
+// dynamic shared memory exceeds the 48 KB a launch gets without the opt-in.
+// The largest opt-in per (kernel, device) is remembered, so the common launch
+// costs one table lookup instead of two driver calls.
+int set_dynamic_smem_fn(const void* kernel, size_t dyn);
+template <class Kern>
+inline int set_dynamic_smem(Kern kernel, size_t dyn) {
+  return set_dynamic_smem_fn(reinterpret_cast<const void*>(kernel), dyn);
+}
+
 // Which grid layout a tile kernel reads or writes.
 enum GridLayout { kInternal = 0, kUser = 1 };
 

@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 
 #include "common.cuh"
 #include "internal.cuh"
@@ -32,6 +33,32 @@ thread_local int g_last_cuda_error = 0;
 int cuda_fail(cudaError_t e) {
   g_last_cuda_error = (int)e;
   return e == cudaErrorMemoryAllocation ? MRN_ERR_NOMEM : MRN_ERR_CUDA;
+}
+
+int set_dynamic_smem_fn(const void* kernel, size_t dyn) {
+  struct Rec {
+    size_t static_bytes;
+    size_t opted;  // largest dynamic size opted into so far
+  };
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, Rec> seen;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e);
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = seen.find({kernel, dev});
+  if (it == seen.end()) {
+    cudaFuncAttributes a;
+    e = cudaFuncGetAttributes(&a, kernel);
+    if (e != cudaSuccess) return cuda_fail(e);
+    it = seen.emplace(std::make_pair(kernel, dev), Rec{a.sharedSizeBytes, 0}).first;
+  }
+  Rec& r = it->second;
+  if (dyn + r.static_bytes <= 48 * 1024 || dyn <= r.opted) return MRN_OK;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+  if (e != cudaSuccess) return cuda_fail(e);
+  r.opted = dyn;
+  return MRN_OK;
 }
 
 __device__ __forceinline__ int find_slice_by_point(const SliceGeom* sl, int ns, int64_t p) {
@@ -408,15 +435,15 @@ int mrn_plan_create(mrn_plan** out, int ndim, int n_slices, const int* im_size,
   P->max_coil = maxc;
 
   // Built-in interpolation tile: 10 cells per edge in 2D (tile + halo as a [cell][coil]
-  // region for 32 coils: three CTAs per SM), 6 in 3D (8-coil groups), 256 in 1D.
+  // region for 32 coils: three CTAs per SM), 4 in 3D (16-coil groups), 256 in 1D.
   int deftile[kMaxDim];
-  for (int i = 0; i < ndim; ++i) deftile[i] = (ndim == 1) ? 256 : (ndim == 2 ? 10 : 6);
+  for (int i = 0; i < ndim; ++i) deftile[i] = (ndim == 1) ? 256 : (ndim == 2 ? 10 : 4);
   for (int i = 0; i < ndim; ++i) P->tile[i] = tile ? tile[i] : deftile[i];
   // gridding tiles: 8x8 in 2D (one warp owns a tile), else the interpolation tile
   for (int i = 0; i < ndim; ++i) P->gtile[i] = (ndim >= 2 && !tile) ? 8 : P->tile[i];
   P->max_chunk = max_chunk > 0 ? max_chunk : (ndim == 2 ? 256 : 1024);
   // one warp grids a 2D tile item alone: shorter items keep warps balanced
-  P->grid_chunk = max_chunk > 0 ? max_chunk : (ndim == 2 ? 256 : 1024);
+  P->grid_chunk = max_chunk > 0 ? max_chunk : (ndim == 2 ? 256 : (ndim == 3 ? 4096 : 1024));
 
   // Slices
   int64_t img = 0, ksp = 0, ugrid = 0, trjo = 0, pts = 0, xo = 0;

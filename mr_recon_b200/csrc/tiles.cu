@@ -717,11 +717,7 @@ static Layout plan_layout(const mrn_plan* P, int kind, bool fast = false) {
 
 template <class K>
 static int prepare(K kernel, size_t smem) {
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return cuda_fail(e);
-  }
-  return MRN_OK;
+  return set_dynamic_smem(kernel, smem);
 }
 
 #define MRN_DISPATCH_G(G_, ...)                     \

@@ -1294,11 +1294,7 @@ k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
 // ---------------------------------------------------------------------------
 template <class Kern>
 static int prep_attr(Kern kernel, size_t smem) {
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return cuda_fail(e);
-  }
-  return MRN_OK;
+  return set_dynamic_smem(kernel, smem);
 }
 
 #define MRN_FAST_G(G_, ...)                                        \
@@ -1389,10 +1385,10 @@ int launch_grid_warp(mrn_plan* P, const float2* ksp, const float* dcf, const flo
 }
 
 // Coil group of the lane-per-coil interpolation: all coils of the widest
-// slice up to 32 lanes (2D) or 8 (3D: a 6^3 tile region with its halo then
+// slice up to 32 lanes (2D) or 16 (3D: a 4^3 tile region with its halo then
 // fits three CTAs per SM), or the caller's coil_group.
 static int interp_reg_sub(const mrn_plan* P, int* cg_out, int* ng_out) {
-  const int cap = P->ndim == 3 ? 8 : 32;
+  const int cap = P->ndim == 3 ? 16 : 32;
   int cg = P->coil_group_req > 0 ? std::min(P->coil_group_req, P->max_coil) : std::min(P->max_coil, cap);
   cg = std::max(1, std::min(cg, 32));
   const int ng = (P->max_coil + cg - 1) / cg;

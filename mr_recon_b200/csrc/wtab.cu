@@ -438,10 +438,8 @@ int launch_interp_tab(mrn_plan* P, const float2* grid, int layout, float2* ksp, 
                       cudaStream_t st) {
   int rc = MRN_OK;
   auto go = [&](auto kern) {
-    if (smem > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) { rc = cuda_fail(e); return; }
-    }
+    rc = set_dynamic_smem(kern, smem);
+    if (rc != MRN_OK) return;
     kern<<<gdim, kThreads, smem, st>>>(P->d_items_i, P->d_slices,
                                        make_int2(P->kb.ntaps[0], P->kb.ntaps[1]), P->d_wmeta_i,
                                        P->d_wtab_i, P->d_perm_i, grid, layout, ksp, scale, temporal,
@@ -472,10 +470,8 @@ int launch_grid_warp_tab(mrn_plan* P, const float2* ksp, const float* dcf, const
   const dim3 gdim((unsigned)P->n_items_grid, (unsigned)ng);
   int rc = MRN_OK;
   auto go = [&](auto kern) {
-    if (smem > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) { rc = cuda_fail(e); return; }
-    }
+    rc = set_dynamic_smem(kern, smem);
+    if (rc != MRN_OK) return;
     kern<<<gdim, 32, smem, st>>>(P->d_items_g, P->d_slices, P->d_wmeta_g, P->d_wtab_g, P->d_perm_g,
                                  ksp, dcf, temporal, grid, layout, scale, cg, pstride);
   };

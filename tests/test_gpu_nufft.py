@@ -231,6 +231,27 @@ def test_plan_decomposition_options_rebind(opts):
     assert rel(Nn(out).reshape(1, C, *im), on.adjoint(y[None], trj[None])) < TOL
 
 
+@pytest.mark.parametrize("itile", [3, 4, 5, 6, 8])
+@pytest.mark.parametrize("C", [1, 5, 12, 16])
+def test_3d_interp_regions_across_shared_memory_sizes(itile, C):
+    """3D lane-per-coil interpolation over tile edges and coil counts whose staged regions span 10 KB to over 100 KB, around
+    the 48 KB a launch gets without the shared-memory opt-in (static
+    coordinate staging included)."""
+    from mr_recon_b200 import _lib
+    rng = np.random.RandomState(itile * 31 + C)
+    im = (24, 20, 28)
+    M = 1500
+    trj = ((rng.rand(M, 3) - 0.5) * np.array(im)).astype(np.float32)
+    img = synth.randn_complex((C, *im), rng)
+    on = O.KBNufftOracle(im, 1.25, 4)
+    p = Plan([im], [M], [C], 1.25, (4.0, 4.0, 4.0), device=DEV)
+    p.set_option(_lib.MRN_OPT_INTERP_TILE, itile)
+    p.set_traj(T(trj))
+    ksp = torch.empty(C * M, dtype=torch.complex64, device=DEV)
+    p.forward(T(img).reshape(-1), ksp)
+    assert rel(Nn(ksp).reshape(1, C, -1), on.forward(img[None], trj[None])) < TOL
+
+
 def test_autotune_keeps_parity_and_caches():
     """The autotuner times candidate decompositions on the bound trajectory,
     leaves the plan bound with the fastest, and reuses the choice for the
