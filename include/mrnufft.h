@@ -118,6 +118,13 @@ int mrn_plan_stats(mrn_plan* plan, int64_t* out4);
 #define MRN_OPT_REG_INTERP 9
 int mrn_plan_set_option(mrn_plan* plan, int option, int value);
 
+/* Kaiser-Bessel beta per dimension for a raw (MRN_PLAN_RAW) plan, beta[0..ndim),
+ * the per-axis kernel parameter sigpy's interpolate/gridding take and the
+ * type-3 NUFFT passes (mr_recon linops.py:258-262, 312-319). Dimensions with
+ * different betas run the generic tile kernels. The trajectory must be bound
+ * again afterwards (MRN_ERR_STATE until then). Non-raw plans: MRN_ERR_ARG. */
+int mrn_plan_set_beta(mrn_plan* plan, const double* beta);
+
 /* Stage timing, a profiling aid with no counterpart in the reference (which
  * only prints wall-clock, recons.py:127-133). When on, every call records a
  * CUDA event pair around each stage on the launching stream (not for use

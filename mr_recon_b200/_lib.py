@@ -57,6 +57,7 @@ SIGNATURES = {
     "mrn_plan_sizes": (_i, [_vp, _pi64]),
     "mrn_plan_stats": (_i, [_vp, _pi64]),
     "mrn_plan_set_option": (_i, [_vp, _i, _i]),
+    "mrn_plan_set_beta": (_i, [_vp, _pd]),
     "mrn_plan_enable_timing": (_i, [_vp, _i]),
     "mrn_plan_timing": (_i, [_vp, _pd, _pi64]),
     "mrn_plan_set_traj": (_i, [_vp, _vp, _vp]),

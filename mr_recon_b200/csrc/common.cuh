@@ -58,12 +58,26 @@ constexpr int kKBTerms = 32;  // terms of the I0 power series kept in KBParams
 
 struct KBParams {
   float radius[kMaxDim];  // W_i / 2
-  float beta;
+  float beta;             // beta of dimension 0 (all dimensions when uniform_beta)
+  float betad[kMaxDim];   // beta per dimension (sigpy-style per-axis kernel parameter)
+  int uniform_beta;       // 1: every dimension uses beta (the fast kernels need this)
   int ntaps[kMaxDim];     // candidate taps floor(W_i) + 1
   float inv_radius[kMaxDim];  // 1 / (W_i / 2)
   int series;             // 1: coef holds the series below to float32 accuracy for this beta
+  int nterms;             // terms the series needs for this beta: a multiple of 4 in [16, kKBTerms]
   float coef[kKBTerms];   // (beta^2 / 4)^k / (k!)^2, k = 0 .. kKBTerms-1
 };
+
+// Horner steps over the coefficients k = 4 blk + 3 .. 4 blk, taken only when
+// the plan keeps that block (a warp-uniform branch on a kernel parameter).
+// Skipped top blocks leave p = 0, so the first kept block starts the
+// recurrence at its highest coefficient.
+#define MRN_KB_HIGH_BLOCKS(STEP)                                   \
+  _Pragma("unroll") for (int blk = kKBTerms / 4 - 1; blk >= 4; --blk) { \
+    if (kb.nterms > 4 * blk) {                                     \
+      _Pragma("unroll") for (int k = 4 * blk + 3; k >= 4 * blk; --k) { STEP; } \
+    }                                                              \
+  }
 
 // Tap weight from |dx| with a precomputed 1/r (the validity test |dx| <= r is
 // done by the caller in float32, exactly as the reference's mask), by the
@@ -91,13 +105,17 @@ __device__ __forceinline__ float kb_tap_as(float adx, float inv_r, float beta) {
 // no cancellation (relative error a few ulp, below the 1e-7 error of the
 // A&S approximations themselves). kKBTerms fused multiply-adds with the
 // coefficients in kernel parameter space: no branch, no special-function
-// unit, no square root.
+// unit, no square root. Only the kb.nterms leading terms are evaluated: the
+// series is positive with terms shrinking faster than geometrically, and the
+// plan picks nterms so the dropped tail at t = 1 (where the relative tail is
+// largest) is below 1e-9 of the sum.
 __device__ __forceinline__ float kb_tap_series(float adx, float inv_r, const KBParams& kb) {
   const float x = adx * inv_r;
   const float t = fmaxf(1.0f - x * x, 0.0f);
-  float w = kb.coef[kKBTerms - 1];
+  float w = 0.0f;
+  MRN_KB_HIGH_BLOCKS(w = fmaf(w, t, kb.coef[k]))
 #pragma unroll
-  for (int k = kKBTerms - 2; k >= 0; --k) w = fmaf(w, t, kb.coef[k]);
+  for (int k = 15; k >= 0; --k) w = fmaf(w, t, kb.coef[k]);
   return w;
 }
 
@@ -108,9 +126,10 @@ __device__ __forceinline__ float kb_tap_series(float adx, float inv_r, const KBP
 __device__ __forceinline__ float2 kb_tap_series_du(float dx, float inv_r, const KBParams& kb) {
   const float x = fabsf(dx) * inv_r;
   const float t = fmaxf(1.0f - x * x, 0.0f);
-  float p = kb.coef[kKBTerms - 1], d = 0.0f;
+  float p = 0.0f, d = 0.0f;
+  MRN_KB_HIGH_BLOCKS(d = fmaf(d, t, p); p = fmaf(p, t, kb.coef[k]))
 #pragma unroll
-  for (int k = kKBTerms - 2; k >= 0; --k) {
+  for (int k = 15; k >= 0; --k) {
     d = fmaf(d, t, p);
     p = fmaf(p, t, kb.coef[k]);
   }

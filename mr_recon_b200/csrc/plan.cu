@@ -238,6 +238,39 @@ static int sort_items_longest_first(Item* d_items, int64_t n, cudaStream_t st) {
 }
 
 // Tile arrays are allocated for the larger of the two tilings.
+// Kernel shape parameters: beta per dimension, and the I0 power series
+// c_k = (beta^2/4)^k / (k!)^2 (in double) that the fast kernels evaluate,
+// which exists only when every dimension has the same beta.
+static void kb_set_beta(KBParams& kb, const double* betas, int ndim) {
+  const double beta = betas[0];
+  kb.beta = (float)beta;
+  kb.uniform_beta = 1;
+  for (int i = 0; i < kMaxDim; ++i) {
+    kb.betad[i] = (float)(i < ndim ? betas[i] : beta);
+    if (i < ndim && (float)betas[i] != kb.beta) kb.uniform_beta = 0;
+  }
+  const double q = beta * beta / 4.0;
+  double c = 1.0, sum = 0.0;
+  for (int k = 0; k < kKBTerms; ++k) {
+    kb.coef[k] = (float)c;
+    sum += c;
+    c *= q / ((double)(k + 1) * (k + 1));
+  }
+  // c now holds the first omitted term; later terms shrink by q / (k+1)^2 each
+  const double ratio = q / ((double)(kKBTerms + 1) * (kKBTerms + 1));
+  const double tail = ratio < 1.0 ? c / (1.0 - ratio) : 1e300;
+  kb.series = tail < 1e-9 * sum ? 1 : 0;
+  // fewest terms (a multiple of 4, at least 16) whose dropped tail is below
+  // 1e-9 of the sum; the tail after term n is bounded by the omitted terms
+  // kept in coef plus the geometric bound above
+  kb.nterms = kKBTerms;
+  for (int n = 16; n < kKBTerms; n += 4) {
+    double t = tail;
+    for (int k = n; k < kKBTerms; ++k) t += (double)kb.coef[k];
+    if (t < 1e-9 * sum) { kb.nterms = n; break; }
+  }
+}
+
 static int64_t tile_capacity(const mrn_plan* P) { return std::max(P->ntiles, P->ngtiles); }
 
 // Interpolation and gridding tilings of every slice, and their global tile ids.
@@ -409,20 +442,10 @@ int mrn_plan_create(mrn_plan** out, int ndim, int n_slices, const int* im_size,
     beta = M_PI * std::sqrt(std::pow(w / oversamp * (oversamp - 0.5), 2) - 0.8);
   }
   P->beta = beta;
-  P->kb.beta = (float)beta;
   {
-    // I0 power series in t = 1 - x^2: c_k = (beta^2/4)^k / (k!)^2, in double
-    const double q = beta * beta / 4.0;
-    double c = 1.0, sum = 0.0;
-    for (int k = 0; k < kKBTerms; ++k) {
-      P->kb.coef[k] = (float)c;
-      sum += c;
-      c *= q / ((double)(k + 1) * (k + 1));
-    }
-    // c now holds the first omitted term; later terms shrink by q / (k+1)^2 each
-    const double ratio = q / ((double)(kKBTerms + 1) * (kKBTerms + 1));
-    const double tail = ratio < 1.0 ? c / (1.0 - ratio) : 1e300;
-    P->kb.series = tail < 1e-9 * sum ? 1 : 0;
+    double betas[kMaxDim];
+    for (int i = 0; i < kMaxDim; ++i) betas[i] = beta;
+    kb_set_beta(P->kb, betas, ndim);
   }
 
   int maxc = 0;
@@ -627,6 +650,17 @@ int mrn_plan_create(mrn_plan** out, int ndim, int n_slices, const int* im_size,
   }
 #undef PK
   *out = P;
+  return MRN_OK;
+}
+
+int mrn_plan_set_beta(mrn_plan* P, const double* beta) {
+  if (!P || !beta || !(P->flags & MRN_PLAN_RAW)) return MRN_ERR_ARG;
+  for (int i = 0; i < P->ndim; ++i)
+    if (!(beta[i] > 0.0)) return MRN_ERR_ARG;
+  kb_set_beta(P->kb, beta, P->ndim);
+  P->beta = beta[0];
+  P->traj_set = false;
+  P->wtab_ok = false;
   return MRN_OK;
 }
 

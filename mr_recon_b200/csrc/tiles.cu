@@ -162,7 +162,7 @@ k_interp(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBPar
       if (active && q < kb.ntaps[i]) {
         const float u = coord_of<D>(c4, i);
         const float adx = fabsf(__fsub_rn((float)(lo[i] + q), u));
-        if (adx <= kb.radius[i]) w = kb_tap(adx, kb.radius[i], kb.beta);
+        if (adx <= kb.radius[i]) w = kb_tap(adx, kb.radius[i], kb.betad[i]);
       }
       ws[t * SLOTS + slot] = w;
     }
@@ -327,7 +327,7 @@ k_grid(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBParam
         const float u = coord_of<D>(c4, i);
         const float adx = fabsf(__fsub_rn((float)(lo[i] + q), u));
         if (adx <= kb.radius[i]) {
-          w = kb_tap(adx, kb.radius[i], kb.beta);
+          w = kb_tap(adx, kb.radius[i], kb.betad[i]);
           const int l = pos_mod(lo[i] + q, g.nos[i]) - f.org[i];
           loc = (l >= 0 && l < f.size[i]) ? l : -1;
         }
@@ -550,8 +550,8 @@ k_traj_grad(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
         const float u = coord_of<D>(c4, i);
         const float dx = __fsub_rn((float)(lo[i] + q), u);
         if (fabsf(dx) <= kb.radius[i]) {
-          w = kb_tap(fabsf(dx), kb.radius[i], kb.beta);
-          d = kb_tap_du(dx, kb.radius[i], kb.beta);
+          w = kb_tap(fabsf(dx), kb.radius[i], kb.betad[i]);
+          d = kb_tap_du(dx, kb.radius[i], kb.betad[i]);
         }
       }
       ws[t * SLOTS + slot] = w;

@@ -1319,7 +1319,7 @@ static int prep_attr(Kern kernel, size_t smem) {
   } while (0)
 
 bool fast_path_ok(const mrn_plan* P, bool gridding) {
-  if (!P->use_fast || P->ndim < 2) return false;
+  if (!P->use_fast || P->ndim < 2 || !P->kb.uniform_beta) return false;
   const int K = P->kb.ntaps[0];
   if (K < 5 || K > 8) return false;
   for (int i = 1; i < P->ndim; ++i)

@@ -65,11 +65,14 @@ def alpha_segementation(phis: torch.Tensor, alphas: torch.Tensor, L: int,
     * b_l(r) = exp(-2 pi i phi(r) alpha_l);
     * interp_type 'zero': h_l(t) = 1 where alpha(t) is nearest alpha_l;
       'lstsq': h = pinv(B^H B / N) (B^H e(t) / N), the least-squares
-      interpolator; the voxel sum (1/N) sum_r conj(b_l(r)) e^{-2 pi i phi(r)
-      alpha(t)}, which the reference takes with a type-3 NUFFT, is evaluated
-      here exactly in float64, once per distinct alpha value (alpha depends
-      on the readout index only), as a chunked matrix product.
-    ``L_batch_size``, ``use_type3`` and ``verbose`` are accepted for interface
+      interpolator. The voxel sums (1/N) sum_r conj(b_l(r)) e^{-2 pi i
+      phi(r) alpha(t)} come, with ``use_type3`` (the reference's default),
+      from the Kaiser-Bessel type-3 NUFFT on the B200 kernels
+      (type3_nufft(phis, alphas).forward, field.py:346-363), else exactly in
+      float64, as type3_nufft_naive would (but once per distinct alpha
+      value, alpha depending on the readout index only, as a chunked matrix
+      product instead of a dense R x T matrix).
+    ``L_batch_size`` and ``verbose`` are accepted for interface
     compatibility."""
     if phis.shape[0] != 1 or alphas.shape[0] != 1:
         raise NotImplementedError("alpha_segementation supports a single phase basis (B = 1)")
@@ -90,15 +93,29 @@ def alpha_segementation(phis: torch.Tensor, alphas: torch.Tensor, L: int,
         phr = ph.reshape(-1).to(torch.float64)
         sp = spatial.reshape(L, -1).to(torch.complex128)
         AHA = (sp.conj() @ sp.T) / n  # AHA[i, j] = mean(conj(b_i) b_j)
-        ua, inv = torch.unique(alphas.reshape(-1).to(torch.float64), return_inverse=True)
-        AHy = torch.zeros((L, ua.numel()), dtype=torch.complex128, device=dev)
-        # (1/N) sum_r conj(b_l(r)) e^{-2 pi i phi(r) alpha}, exact, as a chunked matrix product
-        chunk = max(1, (1 << 24) // max(n, 1))
-        for c0 in range(0, ua.numel(), chunk):
-            e = torch.exp(-2j * math.pi * phr[:, None] * ua[None, c0:c0 + chunk])  # (N, A)
-            AHy[:, c0:c0 + chunk] = (sp.conj() @ e) / n
+        if use_type3:
+            # as the reference (field.py:352-367): Gram matrix, voxel sums and
+            # pinv in complex64, whose default cut-off (L x float32 eps) keeps
+            # the type-3 error (~1e-3) out of the Gram matrix's null space
+            from .linops import type3_nufft
+            t3n = type3_nufft(phis, alphas)
+            s64 = spatial.reshape(L, -1).to(complex_dtype)
+            AHA64 = (s64.conj() @ s64.T) / n
+            AHy = t3n.forward(spatial.conj().to(complex_dtype)).reshape(L, -1) / n
+            h = torch.linalg.pinv(AHA64) @ AHy
+            return spatial, h.reshape((L,) + tuple(trj_size)).to(complex_dtype)
+        else:
+            ua, inv = torch.unique(alphas.reshape(-1).to(torch.float64), return_inverse=True)
+            AHy = torch.zeros((L, ua.numel()), dtype=torch.complex128, device=dev)
+            # (1/N) sum_r conj(b_l(r)) e^{-2 pi i phi(r) alpha}, exact, as a chunked matrix product
+            chunk = max(1, (1 << 24) // max(n, 1))
+            for c0 in range(0, ua.numel(), chunk):
+                e = torch.exp(-2j * math.pi * phr[:, None] * ua[None, c0:c0 + chunk])  # (N, A)
+                AHy[:, c0:c0 + chunk] = (sp.conj() @ e) / n
         h = torch.linalg.pinv(AHA) @ AHy
-        temporal = h[:, inv].reshape((L,) + tuple(trj_size)).to(complex_dtype)
+        if inv is not None:
+            h = h[:, inv]
+        temporal = h.reshape((L,) + tuple(trj_size)).to(complex_dtype)
     else:
         raise NotImplementedError(f"interp_type {interp_type!r}")
     return spatial, temporal

@@ -45,7 +45,7 @@ def _width_tuple(width, ndim):
 
 def _raw_plan(grid_size, nbatch, locs, width, beta):
     npts = locs.numel() // locs.shape[-1]
-    key = ("raw", tuple(grid_size), nbatch, width, float(beta), traj_key(locs))
+    key = ("raw", tuple(grid_size), nbatch, width, beta, traj_key(locs))
 
     def make():
         p = Plan([tuple(grid_size)], [npts], [nbatch], 1.0, width, beta, raw=True, device=locs.device)
@@ -56,9 +56,19 @@ def _raw_plan(grid_size, nbatch, locs, width, beta):
     return _cache.get(key, locs, make)
 
 
-def _beta(kernel_params):
+def _beta(kernel_params, ndim):
+    """kernel_params['beta']: one value (kernels.py:258-265, default 1.0) or,
+    as sigpy's per-axis ``param``, one per dimension."""
     kp = {} if kernel_params is None else kernel_params
-    return float(kp.get("beta", 1.0))  # kernels.py:258-265 default
+    b = kp.get("beta", 1.0)
+    if isinstance(b, torch.Tensor):
+        b = b.tolist()
+    if isinstance(b, (list, tuple)):
+        b = tuple(float(v) for v in b)
+        if len(b) != ndim:
+            raise ValueError(f"kernel_params beta per dimension needs {ndim} values, got {len(b)}")
+        return b[0] if len(set(b)) == 1 else b
+    return float(b)
 
 
 def _ungrid_impl(vals, locs, width, beta):
@@ -151,7 +161,7 @@ def ungrid(vals: torch.Tensor, locs: torch.Tensor, width, kernel: str = "kaiser_
     _lib.require_cuda(vals, "vals")
     _lib.require_cuda(locs, "locs")
     width = _width_tuple(width, locs.shape[-1])
-    beta = _beta(kernel_params)
+    beta = _beta(kernel_params, locs.shape[-1])
     if torch.is_grad_enabled() and (vals.requires_grad or locs.requires_grad):
         return _UngridFn.apply(vals, locs, width, beta)
     return _ungrid_impl(vals, locs, width, beta)
@@ -169,7 +179,7 @@ def grid(vals: torch.Tensor, locs: torch.Tensor, grid_size, width, kernel: str =
         raise ValueError(f"Expected last dim of locs: to equal ndim but got locs.shape[-1] "
                          f"{locs.shape[-1]} != ndim {len(grid_size)}")
     width = _width_tuple(width, len(grid_size))
-    beta = _beta(kernel_params)
+    beta = _beta(kernel_params, len(grid_size))
     if torch.is_grad_enabled() and (vals.requires_grad or locs.requires_grad):
         return _GridFn.apply(vals, locs, grid_size, width, beta)
     return _grid_impl(vals, locs, grid_size, width, beta)

@@ -21,7 +21,8 @@ def _as_arr(vals, ctype):
 
 class Plan:
     """A batch of ``len(im_sizes)`` independent NUFFT problems (slices) that
-    share dimension, kernel width, oversampling and beta."""
+    share dimension, kernel width, oversampling and beta. A raw plan also
+    takes one beta per dimension (a sequence), as sigpy's gridding does."""
 
     def __init__(self, im_sizes: Sequence[Sequence[int]], n_pts: Sequence[int],
                  n_coil: Sequence[int], oversamp: float, width: Sequence[float],
@@ -45,6 +46,14 @@ class Plan:
             raise RuntimeError("mr_recon_b200 plans live on a CUDA device (no CPU fallback)")
         self.device = torch.device("cuda", dev.index if dev.index is not None else torch.cuda.current_device())
         flags = (_lib.MRN_PLAN_RAW if raw else 0) | (0 if apodize else _lib.MRN_PLAN_NO_APOD)
+        beta_d = None
+        if beta is not None and not isinstance(beta, (int, float)):
+            beta_d = [float(b) for b in beta]
+            if len(beta_d) != self.ndim:
+                raise ValueError(f"beta per dimension needs {self.ndim} values, got {len(beta_d)}")
+            if not raw:
+                raise ValueError("beta per dimension is for raw (gridding) plans")
+            beta = beta_d[0]
         flat = [v for s in self.im_sizes for v in s]
         h = C.c_void_p()
         rc = lib.mrn_plan_create(
@@ -55,6 +64,8 @@ class Plan:
             int(coil_group), int(max_chunk), self.device.index)
         check(rc, "mrn_plan_create")
         self.handle = h
+        if beta_d is not None:
+            check(lib.mrn_plan_set_beta(h, _as_arr(beta_d, C.c_double)), "mrn_plan_set_beta")
         check(lib.mrn_plan_set_option(h, _lib.MRN_OPT_FAST_KERNELS, 1 if fast else 0), "mrn_plan_set_option")
         check(lib.mrn_plan_set_option(h, _lib.MRN_OPT_WARP_GRIDDING, 1 if warp_grid else 0),
               "mrn_plan_set_option")

@@ -575,3 +575,133 @@ def cg_sense(A: SenseOracle, ksp, max_iter, lamda_l2, max_eigen, tolerance=1e-8)
         return AHb.astype(C64)
     return conjugate_gradient(lambda v: A.normal(v.astype(C64)).astype(np.complex128) / max_eigen,
                               AHb, num_iters=max_iter, lamda_l2=lamda_l2, tolerance=tolerance)
+
+
+# --------------------------------------------------------------------------
+# Type-3 NUFFT y(t) = sum_r x(r) exp(-2 pi i phi(r) . alpha(t)):
+# type3_nufft_naive (linops.py:49-121) exactly in float64, and the
+# Kaiser-Bessel type-3 of type3_nufft (linops.py:123-425, after Barnett et
+# al.): image-domain gridding of x at the rescaled phis, a type-2 NUFFT of
+# that grid at the rescaled alphas, deapodization, midpoint phases.
+# --------------------------------------------------------------------------
+def type3_naive(x, phis, alphas, chunk=2048):
+    """type3_nufft_naive.forward (linops.py:72-88) in float64: x (N, *im),
+    phis (B, *im), alphas (B, *trj) -> (N, *trj)."""
+    B = phis.shape[0]
+    ph = np.asarray(phis, np.float64).reshape(B, -1)
+    al = np.asarray(alphas, np.float64).reshape(B, -1)
+    N = x.shape[0]
+    xf = np.asarray(x).reshape(N, -1).astype(np.complex128)
+    out = np.zeros((N, al.shape[1]), np.complex128)
+    for t0 in range(0, al.shape[1], chunk):
+        e = np.exp(-2j * np.pi * (ph.T @ al[:, t0:t0 + chunk]))
+        out[:, t0:t0 + chunk] = xf @ e
+    return out.reshape((N,) + alphas.shape[1:])
+
+
+def type3_naive_adjoint(y, phis, alphas, chunk=2048):
+    """type3_nufft_naive.adjoint (linops.py:90-106) in float64."""
+    B = phis.shape[0]
+    ph = np.asarray(phis, np.float64).reshape(B, -1)
+    al = np.asarray(alphas, np.float64).reshape(B, -1)
+    N = y.shape[0]
+    yf = np.asarray(y).reshape(N, -1).astype(np.complex128)
+    out = np.zeros((N, ph.shape[1]), np.complex128)
+    for r0 in range(0, ph.shape[1], chunk):
+        e = np.exp(2j * np.pi * (al.T @ ph[:, r0:r0 + chunk]))
+        out[:, r0:r0 + chunk] = yf @ e
+    return out.reshape((N,) + phis.shape[1:])
+
+
+class Type3Oracle:
+    """Restatement of type3_nufft (linops.py:123-425). Constants are formed
+    in float32 with the reference's operation order (linops.py:170-205); the
+    inner NUFFT is sigpy_nufft's defaults (os 1.25, W 6, fourier.py:730-748),
+    which compute the same transform as triton_nufft, so KBNufftOracle
+    stands in for it; the image-domain gridding/interpolation is sigpy's
+    separable KB with one beta per axis (the same kernel as ``grid`` /
+    ``ungrid`` above)."""
+
+    def __init__(self, phis, alphas, oversamp=2.0, width=4.0, use_toep=False):
+        B = phis.shape[0]
+        self.B = B
+        self.ishape = tuple(phis.shape[1:])
+        self.oshape = tuple(alphas.shape[1:])
+        ph = np.asarray(phis, F32).reshape(B, -1)
+        al = np.asarray(alphas, F32).reshape(B, -1)
+        ph_mp = ((ph.min(1) + ph.max(1)) / F32(2)).astype(F32)
+        al_mp = ((al.min(1) + al.max(1)) / F32(2)).astype(F32)
+        ph_c = (ph - ph_mp[:, None]).astype(F32)
+        al_c = (al - al_mp[:, None]).astype(F32)
+        scales = (np.abs(ph_c).max(1) * F32(2)).astype(F32)
+        ph_c = (ph_c / scales[:, None]).astype(F32)
+        ph_mp = (ph_mp / scales).astype(F32)
+        al_c = (al_c * scales[:, None]).astype(F32)
+        al_mp = (al_mp * scales).astype(F32)
+        self.phis, self.alphas, self.phis_mp, self.alphas_mp = ph_c, al_c, ph_mp, al_mp
+        S = np.abs(al_c).max(1).astype(F32)
+        W = float(width)
+        n_os = np.ceil((F32(2) * S * F32(oversamp) + F32(W)).astype(F32)).astype(np.int64)
+        g_os = (n_os.astype(F32) / np.round((n_os.astype(F32) / F32(oversamp)).astype(F32))).astype(F32)
+        g_N = (n_os.astype(F32) / g_os).astype(F32)
+        self.gamma = (n_os.astype(F32) / (F32(2) * g_os * S)).astype(F32)
+        self.beta = (F32(np.pi) * np.sqrt(((F32(W) / g_os) * (g_os - F32(0.5))) ** 2 - F32(0.8))).astype(F32)
+        self.n_os = tuple(int(v) for v in np.ceil((g_N * g_os).astype(F32)))
+        self.g_N, self.g_os, self.W = g_N, g_os, W
+        self.nft = KBNufftOracle(self.n_os, 1.25, 6)
+        up = np.ceil((g_os * g_N).astype(F32)).astype(F32)
+        self.trj = ((up / g_N) * (ph_c.T * g_N / self.gamma) + np.floor(up / F32(2))).astype(F32)  # (R, B)
+        self.kerns = None
+        if use_toep:
+            w = self._apod() ** 2
+            self.kerns = self.nft.calc_toeplitz_kernels((al_c.T * self.gamma)[None].astype(F32),
+                                                        weights=w[None].astype(F32))
+
+    def _apod(self):
+        x = (self.alphas.T * self.gamma / self.g_N / self.g_os).astype(F32)  # (T, B)
+        a = np.sqrt(self.beta.astype(np.float64) ** 2 - (np.pi * self.W * x.astype(np.float64)) ** 2)
+        return np.prod(a / np.sinh(a), axis=-1)
+
+    def _grid(self, xv):
+        g = grid(xv, self.trj, self.n_os, (self.W,) * self.B, self.beta)
+        return (g / F32(self.W ** self.B)).astype(C64)
+
+    def _interp(self, g):
+        v = ungrid(g, self.trj, (self.W,) * self.B, self.beta)
+        return (v / F32(self.W ** self.B)).astype(C64)
+
+    def forward(self, x):
+        N = x.shape[0]
+        phz = self.phis.T.astype(np.float64) @ self.alphas_mp.astype(np.float64)
+        xm = (np.asarray(x).reshape(N, -1) * np.exp(-2j * np.pi * phz)).astype(C64)
+        xg = self._grid(xm)
+        trj = np.repeat((self.alphas.T * self.gamma)[None].astype(F32), N, 0)
+        y = self.nft.forward(xg, trj).astype(np.complex128) * np.sqrt(np.prod(self.n_os))
+        y = y * self._apod()
+        phz = (self.alphas.T.astype(np.float64) + self.alphas_mp) @ self.phis_mp.astype(np.float64)
+        return (y * np.exp(-2j * np.pi * phz)).astype(C64).reshape((N,) + self.oshape)
+
+    def adjoint(self, y):
+        N = y.shape[0]
+        phz = self.alphas.T.astype(np.float64) @ self.phis_mp.astype(np.float64)
+        ym = np.asarray(y).reshape(N, -1) * np.exp(2j * np.pi * phz) * self._apod()
+        trj = np.repeat((self.alphas.T * self.gamma)[None].astype(F32), N, 0)
+        xg = self.nft.adjoint(ym.astype(C64), trj).astype(np.complex128) * np.sqrt(np.prod(self.n_os))
+        x = self._interp(xg.astype(C64)).astype(np.complex128)
+        phz = (self.phis.T.astype(np.float64) + self.phis_mp) @ self.alphas_mp.astype(np.float64)
+        return (x * np.exp(2j * np.pi * phz)).astype(C64).reshape((N,) + self.ishape)
+
+    def normal(self, x):
+        if self.kerns is None:
+            return self.adjoint(self.forward(x))
+        N = x.shape[0]
+        B = self.B
+        phz = (self.phis.T.astype(np.float64) + self.phis_mp) @ self.alphas_mp.astype(np.float64)
+        xm = (np.asarray(x).reshape(N, -1) * np.exp(-2j * np.pi * phz)).astype(C64)
+        xg = self._grid(xm)
+        ax = tuple(range(-B, 0))
+        xz = resize(xg, (N,) + tuple(2 * n for n in self.n_os))
+        xt = ifft_c(fft_c(xz, axes=ax, norm="ortho") * self.kerns, axes=ax, norm="ortho")
+        xg = (resize(xt, (N,) + self.n_os) * np.prod(self.n_os)).astype(C64)
+        out = self._interp(xg).astype(np.complex128) * np.exp(2j * np.pi * phz)
+        return out.astype(C64).reshape((N,) + self.ishape)

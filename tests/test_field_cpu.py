@@ -55,7 +55,7 @@ def test_lstsq_segmentation_matches_reference():
         return np.linalg.norm(ap - exact) / np.linalg.norm(exact)
 
     for L, tol in ((4, 1e-5), (9, 1e-2)):
-        s, t = alpha_segementation(phis, alphas, L, interp_type="lstsq", verbose=False)
+        s, t = alpha_segementation(phis, alphas, L, interp_type="lstsq", use_type3=False, verbose=False)
         assert rel(s.numpy(), g[f"lstsq{L}_spatial"]) < 1e-6
         assert rel(t.numpy(), g[f"lstsq{L}_temporal"]) < tol
         assert model_err(s.numpy(), t.numpy()) <= model_err(g[f"lstsq{L}_spatial"], g[f"lstsq{L}_temporal"]) * (1 + 1e-6)
@@ -66,7 +66,7 @@ def test_segmented_phase_model_error_falls_with_L():
     exact = torch.exp(-2j * np.pi * phis[0][..., None, None] * alphas[0][None, None])  # (*im, 1, T)
     errs = []
     for L in (2, 4, 8, 16):
-        s, t = alpha_segementation(phis, alphas, L, interp_type="lstsq", verbose=False)
+        s, t = alpha_segementation(phis, alphas, L, interp_type="lstsq", use_type3=False, verbose=False)
         approx = torch.einsum("lxy,lat->xyat", s, t)
         errs.append(rel(approx.numpy(), exact.numpy()))
     assert all(b < a for a, b in zip(errs, errs[1:])) and errs[-1] < 1e-3

@@ -520,3 +520,68 @@ def test_density_compensation_pipe_menon_properties():
     mid = d[(r > 14) & (r < 20)].mean()
     outer = d[(r > 24) & (r < 30)].mean()
     assert float(inner) < float(mid) < float(outer)
+
+
+# ----------------------------------------------------------------- type-3 NUFFT
+def test_raw_grid_per_axis_beta_matches_oracle():
+    """Gridding / interpolation with one KB beta per axis (sigpy's per-axis
+    kernel parameter, which type3_nufft passes) against the oracle."""
+    rng = np.random.RandomState(41)
+    gs, betas = (31, 24), (8.9, 7.3)
+    locs = (rng.rand(1500, 2) * np.array(gs)).astype(np.float32)
+    vals = synth.randn_complex((3, 1500), rng)
+    gvals = synth.randn_complex((3, *gs), rng)
+    kp = {"beta": betas}
+    g = mgrid(T(vals), T(locs), gs, (4.0, 4.0), kernel_params=kp)
+    u = mungrid(T(gvals), T(locs), (4.0, 4.0), kernel_params=kp)
+    b = np.array(betas, np.float32)
+    assert rel(Nn(g), O.grid(vals, locs, gs, (4.0, 4.0), b)) < TOL
+    assert rel(Nn(u), O.ungrid(gvals, locs, (4.0, 4.0), b)) < TOL
+
+
+@pytest.mark.parametrize("tag", ["b1", "b2"])
+def test_type3_nufft_matches_oracle(tag):
+    """type3_nufft on the B200 kernels against the oracle's restatement of
+    the reference's KB type-3 (same algorithm: 1e-4, the midpoint phases
+    being formed in float32 here and float64 there) and against the
+    reference's exact sums (the kernel's accuracy, 3e-3)."""
+    from mr_recon_b200.linops import type3_nufft
+    g = load("type3.npz")
+    ph, al = g[f"{tag}_phis"], g[f"{tag}_alphas"]
+    x, y = g[f"{tag}_x"], g[f"{tag}_y"]
+    op = type3_nufft(T(ph), T(al))
+    on = O.Type3Oracle(ph, al)
+    assert op.grd_N_os == on.n_os
+    f = Nn(op.forward(T(x)))
+    a = Nn(op.adjoint(T(y)))
+    assert rel(f, on.forward(x)) < 1e-4
+    assert rel(a, on.adjoint(y)) < 1e-4
+    assert rel(f, g[f"{tag}_fwd"]) < 3e-3
+    assert rel(a, g[f"{tag}_adj"]) < 3e-3
+    assert rel(Nn(op.normal(T(x))), on.adjoint(on.forward(x))) < 1e-4
+    opt = type3_nufft(T(ph), T(al), use_toep=True)
+    ont = O.Type3Oracle(ph, al, use_toep=True)
+    assert rel(Nn(opt.kerns), ont.kerns) < 1e-4
+    assert rel(Nn(opt.normal(T(x))), ont.normal(x)) < 1e-4
+
+
+def test_alpha_segmentation_lstsq_type3_vs_exact():
+    """alpha_segementation's least-squares temporal functions through the
+    type-3 NUFFT (the reference's default): with a well-conditioned Gram
+    matrix (L = 4) they agree with the exact voxel sums; at larger L the
+    phase model stays within the type-3 accuracy (the reference's own
+    behaviour, its complex64 pinv cutting the null space)."""
+    from mr_recon_b200.field import alpha_segementation, b0_to_phis_alphas
+    im = (36, 32)
+    yy, xx = np.meshgrid(np.linspace(-1, 1, im[0]), np.linspace(-1, 1, im[1]), indexing="ij")
+    b0 = (70 * xx + 40 * yy ** 2 + 90 * np.exp(-((xx + 0.2) ** 2 + yy ** 2) / 0.08)).astype(np.float32)
+    phis, alphas = b0_to_phis_alphas(T(b0), (2, 300), 1, 12e-3 / 300)
+    exact = np.exp(-2j * np.pi * Nn(phis)[0][..., None, None].astype(np.float64) * Nn(alphas)[0][None, None])
+    for L in (4, 8, 12):
+        s3, t3 = alpha_segementation(phis, alphas, L, interp_type="lstsq", use_type3=True, verbose=False)
+        se, te = alpha_segementation(phis, alphas, L, interp_type="lstsq", use_type3=False, verbose=False)
+        if L == 4:
+            assert rel(Nn(t3), Nn(te)) < 1e-3
+        m3 = rel(np.einsum("lxy,lat->xyat", Nn(s3), Nn(t3)), exact)
+        me = rel(np.einsum("lxy,lat->xyat", Nn(se), Nn(te)), exact)
+        assert m3 < me * 1.05 + 2e-3

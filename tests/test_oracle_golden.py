@@ -117,3 +117,31 @@ def test_image_gradient_matches_reference_autograd():
     r = nf.forward(g["ag_img"], g["ag_trj"]) - g["ag_y"]
     grad = 2 * nf.adjoint(r.astype(np.complex64), g["ag_trj"])
     assert rel(grad, g["ag_grad"]) < 1e-5
+
+
+# ----------------------------------------------------------------- type-3
+@pytest.mark.parametrize("tag", ["b1", "b2"])
+def test_type3_naive_matches_reference(tag):
+    """The float64 naive type-3 sum against the reference's own
+    type3_nufft_naive (float32 there, so 1e-5)."""
+    g = load("type3.npz")
+    ph, al = g[f"{tag}_phis"], g[f"{tag}_alphas"]
+    assert rel(O.type3_naive(g[f"{tag}_x"], ph, al), g[f"{tag}_fwd"]) < 1e-5
+    assert rel(O.type3_naive_adjoint(g[f"{tag}_y"], ph, al), g[f"{tag}_adj"]) < 1e-5
+
+
+@pytest.mark.parametrize("tag", ["b1", "b2"])
+def test_type3_kb_restatement_against_reference_sums(tag):
+    """The Kaiser-Bessel type-3 restatement (os 2, W 4) reproduces the
+    reference's exact sums to the accuracy of the kernel (a wrong scale,
+    shift or phase convention would give O(1) errors); B = 2 has a
+    different oversampling, hence beta, per axis."""
+    g = load("type3.npz")
+    ph, al = g[f"{tag}_phis"], g[f"{tag}_alphas"]
+    t3 = O.Type3Oracle(ph, al)
+    if tag == "b2":
+        assert t3.beta[0] != t3.beta[1]
+    assert rel(t3.forward(g[f"{tag}_x"]), g[f"{tag}_fwd"]) < 3e-3
+    assert rel(t3.adjoint(g[f"{tag}_y"]), g[f"{tag}_adj"]) < 3e-3
+    exact = O.type3_naive_adjoint(g[f"{tag}_fwd"], ph, al)
+    assert rel(O.Type3Oracle(ph, al, use_toep=True).normal(g[f"{tag}_x"]), exact) < 3e-3
