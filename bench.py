@@ -165,13 +165,20 @@ def bench_c3(dev, steps, peak, N=192, spokes=20000):
     plan.enable_timing(True)
     plan.timing()
     e0, e1 = _events(torch)
+    sev = [_events(torch) for _ in range(steps)]
+    host_s = 0.0
     e0.record()
-    for _ in range(steps):
+    for i in range(steps):
+        sev[i][0].record()
+        h0 = time.perf_counter()
         k = nf.forward(img, trj)
         nf.adjoint(k, trj)
+        host_s += time.perf_counter() - h0
+        sev[i][1].record()
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
+    step_ms = [a.elapsed_time(b) for a, b in sev]
     st = plan.timing()
     plan.enable_timing(False)
     Gos = int(math.ceil(1.25 * N)) ** 3
@@ -211,6 +218,7 @@ def bench_c3(dev, steps, peak, N=192, spokes=20000):
         "interp_roofline": {"achieved": alg / (i_ms / 1e3) / 1e9, "frac": alg / (i_ms / 1e3) / 1e9 / peak,
                             "kernel_ms": i_ms},
         "autograd_step_ms": ag_ms, "autograd_stage_ms": ag_stage, "plan_setup_s": setup_s, "plan": stats,
+        "step_ms_each": step_ms, "host_enqueue_ms_per_step": host_s * 1e3 / steps,
     }
 
 

@@ -1106,17 +1106,19 @@ k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBP
 // ---------------------------------------------------------------------------
 // 3D gridding with the tile accumulator in registers. One CTA of 8 warps per
 // work item and group of at most 16 coils; the tile is at most 8x8x8 cells.
-// Warp w owns x-plane w, half-warp h owns y-rows 4h..4h+3, lane = coil, so
-// each thread keeps 4 (y) x 8 (z) complex cells in registers. Same pipeline
-// as the 2D kernel (coordinates through a cp.async ring, tile-aligned 1D
-// weights computed once per entry in shared memory, sample values copied
-// asynchronously one batch ahead); per entry a warp whose x-plane has zero
-// weight skips it, and every y-row with a weight takes 8 packed two-lane
-// FMAs along z. No atomics except for split tiles' write-back; float32
-// accumulation in a fixed order.
+// Warp w owns x-plane w, half-warp h owns z-cells 4h..4h+3, lane = coil, so
+// each thread keeps 8 (y) x 4 (z) complex cells in registers and the y-rows
+// are the same for the whole warp (a row without weight is skipped by a
+// warp-uniform branch). Same pipeline as the 2D kernel (coordinates through
+// a cp.async ring, tile-aligned 1D weights computed once per entry in shared
+// memory, sample values copied asynchronously one batch ahead), in batches
+// of 64 entries; per batch each warp takes one ballot of the entries whose
+// footprint meets its x-plane and visits only those. Every y-row with a
+// weight takes 4 packed two-lane FMAs along z. No atomics except for split
+// tiles' write-back; float32 accumulation in a fixed order.
 // ---------------------------------------------------------------------------
 constexpr int kReg3Tile = 8;
-constexpr int kReg3Batch = 32;
+constexpr int kReg3Batch = 64;
 constexpr int kReg3Coils = 16;
 
 template <int K>
@@ -1154,7 +1156,7 @@ k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
   auto copy_coords = [&](int bi) {
     const int nb = batch_len(bi), r3 = bi % 3;
     if (tid < nb) cp_async16(&s_c[r3][tid], coord + it.start + bi * B + tid);
-    else if (tid >= 32 && tid - 32 < nb) cp_async4(&s_pm[r3][tid - 32], perm + it.start + bi * B + tid - 32);
+    else if (tid >= B && tid - B < nb) cp_async4(&s_pm[r3][tid - B], perm + it.start + bi * B + tid - B);
   };
   // thread = (entry j and j + 16, coil c): one 8-byte copy per entry and coil
   auto copy_values = [&](int bi) {
@@ -1165,47 +1167,49 @@ k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
       if (j < nb && c < ncg) cp_async8(&s_v[b2][j][c], kspg + (int64_t)c * m + (s_pm[r3][j] - pt_off));
     if (tid < nb) {
       if (dcf) cp_async4(&s_d[b2][tid], dcf + s_pm[r3][tid]);
-    } else if (tid >= 32 && tid - 32 < nb) {
-      if (temporal) cp_async8(&s_t[b2][tid - 32], temporal + s_pm[r3][tid - 32]);
+    } else if (tid >= B && tid - B < nb) {
+      if (temporal) cp_async8(&s_t[b2][tid - B], temporal + s_pm[r3][tid - B]);
     }
   };
-  // thread < 6 B = (entry j, dimension i, half hh): tile-aligned weights of 4 cells
+  // work unit t < 6 B = (entry j, dimension i, half hh), strided over the CTA:
+  // tile-aligned weights of 4 cells
   auto weights = [&](int bi) {
-    if (tid >= 6 * B) return;
-    const int pair = tid >> 1, hh = tid & 1;
-    const int j = pair / 3, i = pair - 3 * j;
-    if (j >= batch_len(bi)) return;
-    const float4 c4 = s_c[bi % 3][j];
-    const float u = i == 0 ? c4.x : (i == 1 ? c4.y : c4.z);
-    const float r = sel3(kb.radius, i), ir = sel3(kb.inv_radius, i);
-    const int n = sel3(gp->nos, i), size = sel3(f.size, i);
-    const int lo = (int)ceilf(__fsub_rn(u, r));
-    int st = wrap_once(lo, n) - sel3(f.org, i);
-    if (st >= size) st -= n;  // footprint wraps into this tile from the end
-    float w[4];
+    for (int t = tid; t < 6 * B; t += 256) {
+      const int pair = t >> 1, hh = t & 1;
+      const int j = pair / 3, i = pair - 3 * j;
+      if (j >= batch_len(bi)) continue;
+      const float4 c4 = s_c[bi % 3][j];
+      const float u = i == 0 ? c4.x : (i == 1 ? c4.y : c4.z);
+      const float r = sel3(kb.radius, i), ir = sel3(kb.inv_radius, i);
+      const int n = sel3(gp->nos, i), size = sel3(f.size, i);
+      const int lo = (int)ceilf(__fsub_rn(u, r));
+      int st = wrap_once(lo, n) - sel3(f.org, i);
+      if (st >= size) st -= n;  // footprint wraps into this tile from the end
+      float w[4];
 #pragma unroll
-    for (int l = 0; l < 4; ++l) {
-      const int cell = 4 * hh + l;
-      const int q = cell - st;
-      const float adx = fabsf(__fsub_rn((float)(lo + q), u));
-      w[l] = (q >= 0 && q < K && cell < size && adx <= r) ? kb_tap_fast(adx, ir, kb) : 0.f;
-    }
-    const int b2 = bi & 1;
-    if (i == 0) {
-      s_wx[b2][j][hh] = make_float4(w[0] * scale, w[1] * scale, w[2] * scale, w[3] * scale);
-    } else if (i == 1) {
-      s_wy[b2][j][hh] = make_float4(w[0], w[1], w[2], w[3]);
-    } else {
-      s_wz[b2][j][2 * hh] = make_float4(w[0], w[0], w[1], w[1]);
-      s_wz[b2][j][2 * hh + 1] = make_float4(w[2], w[2], w[3], w[3]);
+      for (int l = 0; l < 4; ++l) {
+        const int cell = 4 * hh + l;
+        const int q = cell - st;
+        const float adx = fabsf(__fsub_rn((float)(lo + q), u));
+        w[l] = (q >= 0 && q < K && cell < size && adx <= r) ? kb_tap_fast(adx, ir, kb) : 0.f;
+      }
+      const int b2 = bi & 1;
+      if (i == 0) {
+        s_wx[b2][j][hh] = make_float4(w[0] * scale, w[1] * scale, w[2] * scale, w[3] * scale);
+      } else if (i == 1) {
+        s_wy[b2][j][hh] = make_float4(w[0], w[1], w[2], w[3]);
+      } else {
+        s_wz[b2][j][2 * hh] = make_float4(w[0], w[0], w[1], w[1]);
+        s_wz[b2][j][2 * hh + 1] = make_float4(w[2], w[2], w[3], w[3]);
+      }
     }
   };
 
-  float2 acc[4][T];
+  float2 acc[8][4];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < 8; ++a)
 #pragma unroll
-    for (int b = 0; b < T; ++b) acc[a][b] = make_float2(0.f, 0.f);
+    for (int b = 0; b < 4; ++b) acc[a][b] = make_float2(0.f, 0.f);
 
   copy_coords(0);
   copy_coords(1);
@@ -1227,34 +1231,41 @@ k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
     cp_async_commit();
     weights(bi + 1);
     const int b2 = bi & 1, nb = batch_len(bi);
-    for (int j = 0; j < nb; ++j) {
-      const float wxv = wxw[(b2 * B + j) * 8 + warp];
-      if (wxv == 0.f) continue;  // uniform: this warp's x-plane is outside the footprint
-      const float4 wy4 = s_wy[b2][j][half];
-      const float wy[4] = {wy4.x, wy4.y, wy4.z, wy4.w};
-      float2 wz[T];
+#pragma unroll 1
+    for (int h32 = 0; h32 < B; h32 += 32) {
+      // entries whose footprint meets this warp's x-plane: one ballot per 32 entries
+      unsigned act = __ballot_sync(0xffffffffu, h32 + lane < nb && wxw[(b2 * B + h32 + lane) * 8 + warp] != 0.f);
+      while (act) {
+        const int j = h32 + __ffs(act) - 1;
+        act &= act - 1u;
+        const float wxv = wxw[(b2 * B + j) * 8 + warp];
+        const float4 wy0 = s_wy[b2][j][0], wy1 = s_wy[b2][j][1];
+        const float wy[8] = {wy0.x, wy0.y, wy0.z, wy0.w, wy1.x, wy1.y, wy1.z, wy1.w};
+        float2 wz[4];
+        {
+          const float4 c0 = s_wz[b2][j][2 * half], c1 = s_wz[b2][j][2 * half + 1];
+          wz[0] = make_float2(c0.x, c0.y);
+          wz[1] = make_float2(c0.z, c0.w);
+          wz[2] = make_float2(c1.x, c1.y);
+          wz[3] = make_float2(c1.z, c1.w);
+        }
+        float2 val = s_v[b2][j][coil];
+        if (dcf) {
+          const float d = s_d[b2][j];
+          val = make_float2(val.x * d, val.y * d);
+        }
+        if (temporal) {  // times conj(t)
+          const float2 t = s_t[b2][j];
+          val = make_float2(val.x * t.x + val.y * t.y, val.y * t.x - val.x * t.y);
+        }
+        val = make_float2(wxv * val.x, wxv * val.y);
 #pragma unroll
-      for (int b = 0; b < T / 2; ++b) {
-        const float4 c = s_wz[b2][j][b];
-        wz[2 * b] = make_float2(c.x, c.y);
-        wz[2 * b + 1] = make_float2(c.z, c.w);
-      }
-      float2 val = s_v[b2][j][coil];
-      if (dcf) {
-        const float d = s_d[b2][j];
-        val = make_float2(val.x * d, val.y * d);
-      }
-      if (temporal) {  // times conj(t)
-        const float2 t = s_t[b2][j];
-        val = make_float2(val.x * t.x + val.y * t.y, val.y * t.x - val.x * t.y);
-      }
-      val = make_float2(wxv * val.x, wxv * val.y);
+        for (int a = 0; a < 8; ++a) {
+          if (wy[a] == 0.f) continue;  // uniform: the whole warp shares the rows
+          const float2 v2 = make_float2(wy[a] * val.x, wy[a] * val.y);
 #pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        if (wy[a] == 0.f) continue;
-        const float2 v2 = make_float2(wy[a] * val.x, wy[a] * val.y);
-#pragma unroll
-        for (int b = 0; b < T; ++b) acc[a][b] = __ffma2_rn(wz[b], v2, acc[a][b]);
+          for (int b = 0; b < 4; ++b) acc[a][b] = __ffma2_rn(wz[b], v2, acc[a][b]);
+        }
       }
     }
   }
@@ -1269,14 +1280,14 @@ k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
   const int64_t xo = (int64_t)wrap_once(f.org[0] + warp - hs0, nos0) * nos1;
   const int z0 = wrap_once(f.org[2] - hs2, nos2);
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    const int y = 4 * half + a;
+  for (int a = 0; a < 8; ++a) {
+    const int y = a;
     if (y >= f.size[1]) break;
     float2* rowp = dst + (xo + wrap_once(f.org[1] + y - hs1, nos1)) * nos2;
 #pragma unroll
-    for (int b = 0; b < T; ++b) {
-      if (b >= f.size[2]) break;
-      int z = z0 + b;
+    for (int b = 0; b < 4; ++b) {
+      if (4 * half + b >= f.size[2]) break;
+      int z = z0 + 4 * half + b;
       if (z >= nos2) z -= nos2;
       float2* d = rowp + z;
       if (it.split) {
