@@ -618,8 +618,48 @@ __device__ __forceinline__ void load_region_cc(float2* __restrict__ region, cons
 constexpr int kRegInterpWarps = 8;
 constexpr int kInterpStage = 128;  // samples whose coordinates are staged at once
 
+// Separable gather of one sample from the [cell][coil] region over the first
+// KE taps of each axis (KE = K, or K - 1 when no axis has its last candidate
+// tap inside the support, which holds unless a coordinate sits exactly W/2
+// from that tap: the skipped terms have weight exactly zero).
+template <int D, int K, int KE, int SUB>
+__device__ __forceinline__ float2 interp_gather(const float2* rb, int inner, int ext1, int CS,
+                                                const float (&w)[D][K], const float2 (&wl)[K]) {
+  float2 acc = make_float2(0.f, 0.f);
+  if (D == 2) {
+#pragma unroll
+    for (int a = 0; a < KE; ++a) {
+      if (SUB == 1 && w[0][a] == 0.f) continue;
+      const float2* rp = rb + a * inner * CS;
+      float2 ra = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int b = 0; b < KE; ++b) ra = __ffma2_rn(wl[b], rp[b * CS], ra);
+      acc = __ffma2_rn(make_float2(w[0][a], w[0][a]), ra, acc);
+    }
+  } else {
+#pragma unroll
+    for (int a = 0; a < KE; ++a) {
+      float2 pa = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int b = 0; b < KE; ++b) {
+        const float2* rp = rb + (a * ext1 + b) * inner * CS;
+        float2 ra = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int c = 0; c < KE; ++c) ra = __ffma2_rn(wl[c], rp[c * CS], ra);
+        pa = __ffma2_rn(make_float2(w[D > 2 ? 1 : 0][b], w[D > 2 ? 1 : 0][b]), ra, pa);
+      }
+      acc = __ffma2_rn(make_float2(w[0][a], w[0][a]), pa, acc);
+    }
+  }
+  return acc;
+}
+
+// Register budget: three CTAs per SM (80 registers) except 3D with six or more
+// taps (two); the two gather paths would otherwise raise register use and
+// lower occupancy (a 2D 10^2 or 3D 4^3 tile region takes ~70 KB of shared
+// memory, so three CTAs fit).
 template <int D, int K, int SUB>
-__global__ void __launch_bounds__(kRegInterpWarps * 32)
+__global__ void __launch_bounds__(kRegInterpWarps * 32, (D == 3 && K > 5) ? 2 : 3)
 k_interp_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBParams kb,
              const float4* __restrict__ coord, const int* __restrict__ perm,
              const float2* __restrict__ grid, int layout, float2* __restrict__ ksp, float scale,
@@ -680,34 +720,13 @@ k_interp_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, K
       float2 wl[K];  // last-axis weights, each twice
 #pragma unroll
       for (int b = 0; b < K; ++b) wl[b] = make_float2(w[D - 1][b], w[D - 1][b]);
-      float2 acc = make_float2(0.f, 0.f);
-      if (D == 2) {
-        const float2* rb = region + (l0[0] * inner + l0[1]) * CS + coil;
+      const float2* rb = D == 2 ? region + (l0[0] * inner + l0[1]) * CS + coil
+                                : region + ((l0[0] * ext[1] + l0[1]) * inner + l0[D - 1]) * CS + coil;
+      bool last = false;  // some axis has its K-th candidate tap inside the support
 #pragma unroll
-        for (int a = 0; a < K; ++a) {
-          if (SUB == 1 && w[0][a] == 0.f) continue;
-          const float2* rp = rb + a * inner * CS;
-          float2 ra = make_float2(0.f, 0.f);
-#pragma unroll
-          for (int b = 0; b < K; ++b) ra = __ffma2_rn(wl[b], rp[b * CS], ra);
-          acc = __ffma2_rn(make_float2(w[0][a], w[0][a]), ra, acc);
-        }
-      } else {
-        const float2* rb = region + ((l0[0] * ext[1] + l0[1]) * inner + l0[D - 1]) * CS + coil;
-#pragma unroll
-        for (int a = 0; a < K; ++a) {
-          float2 pa = make_float2(0.f, 0.f);
-#pragma unroll
-          for (int b = 0; b < K; ++b) {
-            const float2* rp = rb + (a * ext[1] + b) * inner * CS;
-            float2 ra = make_float2(0.f, 0.f);
-#pragma unroll
-            for (int c = 0; c < K; ++c) ra = __ffma2_rn(wl[c], rp[c * CS], ra);
-            pa = __ffma2_rn(make_float2(w[D > 2 ? 1 : 0][b], w[D > 2 ? 1 : 0][b]), ra, pa);
-          }
-          acc = __ffma2_rn(make_float2(w[0][a], w[0][a]), pa, acc);
-        }
-      }
+      for (int i = 0; i < D; ++i) last |= w[i][K - 1] != 0.f;
+      const float2 acc = last ? interp_gather<D, K, K, SUB>(rb, inner, ext[1], CS, w, wl)
+                              : interp_gather<D, K, K - 1, SUB>(rb, inner, ext[1], CS, w, wl);
       const int lp = s_p[el];
       float2 h = make_float2(scale, 0.f);
       if (temporal) {
