@@ -745,6 +745,56 @@ k_interp_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, K
   }
 }
 
+// Separable sums of the trajectory gradient over the first KE taps of each
+// axis (see interp_gather): out[i] = sum over taps of the region value times
+// the weights with axis i's factor replaced by its derivative.
+template <int D, int K, int KE>
+__device__ __forceinline__ void trajgrad_gather(const float2* rb, int inner, int ext1, int CS,
+                                                const float (&w)[D][K], const float (&dw)[D][K],
+                                                float2 (&out)[3]) {
+  float2 a0 = make_float2(0.f, 0.f), a1 = a0, a2 = a0;
+  if (D == 2) {
+#pragma unroll
+    for (int a = 0; a < KE; ++a) {
+      const float2* rp = rb + a * inner * CS;
+      float2 r = make_float2(0.f, 0.f), rd = r;
+#pragma unroll
+      for (int b = 0; b < KE; ++b) {
+        const float2 gv = rp[b * CS];
+        r = __ffma2_rn(make_float2(w[D - 1][b], w[D - 1][b]), gv, r);
+        rd = __ffma2_rn(make_float2(dw[D - 1][b], dw[D - 1][b]), gv, rd);
+      }
+      a0 = __ffma2_rn(make_float2(dw[0][a], dw[0][a]), r, a0);
+      a1 = __ffma2_rn(make_float2(w[0][a], w[0][a]), rd, a1);
+    }
+  } else {
+#pragma unroll
+    for (int a = 0; a < KE; ++a) {
+      float2 p = make_float2(0.f, 0.f), p1 = p, p2 = p;
+#pragma unroll
+      for (int b = 0; b < KE; ++b) {
+        const float2* rp = rb + (a * ext1 + b) * inner * CS;
+        float2 r = make_float2(0.f, 0.f), rd = r;
+#pragma unroll
+        for (int c = 0; c < KE; ++c) {
+          const float2 gv = rp[c * CS];
+          r = __ffma2_rn(make_float2(w[D - 1][c], w[D - 1][c]), gv, r);
+          rd = __ffma2_rn(make_float2(dw[D - 1][c], dw[D - 1][c]), gv, rd);
+        }
+        p = __ffma2_rn(make_float2(w[D > 2 ? 1 : 0][b], w[D > 2 ? 1 : 0][b]), r, p);
+        p1 = __ffma2_rn(make_float2(dw[D > 2 ? 1 : 0][b], dw[D > 2 ? 1 : 0][b]), r, p1);
+        p2 = __ffma2_rn(make_float2(w[D > 2 ? 1 : 0][b], w[D > 2 ? 1 : 0][b]), rd, p2);
+      }
+      a0 = __ffma2_rn(make_float2(dw[0][a], dw[0][a]), p, a0);
+      a1 = __ffma2_rn(make_float2(w[0][a], w[0][a]), p1, a1);
+      a2 = __ffma2_rn(make_float2(w[0][a], w[0][a]), p2, a2);
+    }
+  }
+  out[0] = a0;
+  out[1] = a1;
+  out[2] = a2;
+}
+
 // ---------------------------------------------------------------------------
 // Trajectory gradient, lane = coil: d/du_i Re sum_c conj(S_c) (A x)_c at each
 // sample, the same region staging and sample loop as k_interp_reg. Per
@@ -847,46 +897,15 @@ k_trajgrad_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl,
         }
       float g[3] = {0.f, 0.f, 0.f};
       if (active && has_coil) {
-        float2 a0 = make_float2(0.f, 0.f), a1 = a0, a2 = a0;
-        if (D == 2) {
-          const float2* rb = region + (l0[0] * inner + l0[1]) * CS + coil;
+        float2 acc3[3];
+        const float2* rb = D == 2 ? region + (l0[0] * inner + l0[1]) * CS + coil
+                                  : region + ((l0[0] * ext[1] + l0[1]) * inner + l0[D - 1]) * CS + coil;
+        bool last = false;  // some axis has its K-th candidate tap inside the support
 #pragma unroll
-          for (int a = 0; a < K; ++a) {
-            const float2* rp = rb + a * inner * CS;
-            float2 r = make_float2(0.f, 0.f), rd = r;
-#pragma unroll
-            for (int b = 0; b < K; ++b) {
-              const float2 gv = rp[b * CS];
-              r = __ffma2_rn(make_float2(w[1][b], w[1][b]), gv, r);
-              rd = __ffma2_rn(make_float2(dw[1][b], dw[1][b]), gv, rd);
-            }
-            a0 = __ffma2_rn(make_float2(dw[0][a], dw[0][a]), r, a0);
-            a1 = __ffma2_rn(make_float2(w[0][a], w[0][a]), rd, a1);
-          }
-        } else {
-          const float2* rb = region + ((l0[0] * ext[1] + l0[1]) * inner + l0[D - 1]) * CS + coil;
-#pragma unroll
-          for (int a = 0; a < K; ++a) {
-            float2 p = make_float2(0.f, 0.f), p1 = p, p2 = p;
-#pragma unroll
-            for (int b = 0; b < K; ++b) {
-              const float2* rp = rb + (a * ext[1] + b) * inner * CS;
-              float2 r = make_float2(0.f, 0.f), rd = r;
-#pragma unroll
-              for (int c = 0; c < K; ++c) {
-                const float2 gv = rp[c * CS];
-                r = __ffma2_rn(make_float2(w[D - 1][c], w[D - 1][c]), gv, r);
-                rd = __ffma2_rn(make_float2(dw[D - 1][c], dw[D - 1][c]), gv, rd);
-              }
-              p = __ffma2_rn(make_float2(w[1][b], w[1][b]), r, p);
-              p1 = __ffma2_rn(make_float2(dw[1][b], dw[1][b]), r, p1);
-              p2 = __ffma2_rn(make_float2(w[1][b], w[1][b]), rd, p2);
-            }
-            a0 = __ffma2_rn(make_float2(dw[0][a], dw[0][a]), p, a0);
-            a1 = __ffma2_rn(make_float2(w[0][a], w[0][a]), p1, a1);
-            a2 = __ffma2_rn(make_float2(w[0][a], w[0][a]), p2, a2);
-          }
-        }
+        for (int i = 0; i < D; ++i) last |= w[i][K - 1] != 0.f;
+        if (last) trajgrad_gather<D, K, K>(rb, inner, ext[1], CS, w, dw, acc3);
+        else trajgrad_gather<D, K, K - 1>(rb, inner, ext[1], CS, w, dw, acc3);
+        const float2 a0 = acc3[0], a1 = acc3[1], a2 = acc3[2];
         // Re(conj(S) * acc)
         g[0] = sv.x * a0.x + sv.y * a0.y;
         g[1] = sv.x * a1.x + sv.y * a1.y;
