@@ -45,8 +45,8 @@ WORKLOAD = "2D multi-coil KB NUFFT fwd+adj: 256x256 c64, 32 coils, VD spiral 48x
 # DRAM bytes (read + write) per launch of each tile kernel on this workload,
 # from one ncu capture (profiles/grid_interp_kernels_spiral256_c32.md).
 HOST_AHEAD_S = 0.4e-3  # device-side wait before each timed step: longer than the host's enqueue of one step
-GRID_TRAFFIC_BYTES = 33_542_912 + 44_800
-INTERP_TRAFFIC_BYTES = 25_538_560 + 97_792
+GRID_TRAFFIC_BYTES = 33_565_440 + 60_928
+INTERP_TRAFFIC_BYTES = 26_191_360 + 1_033_728
 
 
 def load_peaks():
