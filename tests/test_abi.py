@@ -73,4 +73,31 @@ def test_null_plan_calls_fail_cleanly():
     assert lib.mrn_adjoint(None, None, None, None) == _lib.MRN_ERR_ARG
     assert lib.mrn_plan_set_traj(None, None, None) == _lib.MRN_ERR_ARG
     assert lib.mrn_plan_destroy(None) == _lib.MRN_OK
+    betas = (C.c_double * 3)(8.0, 7.0, 6.0)
+    assert lib.mrn_plan_set_beta(None, betas) == _lib.MRN_ERR_ARG
     assert lib.mrn_cg_step(None, None, None, None, None, None, None) == _lib.MRN_ERR_ARG
+
+
+def test_per_axis_beta_arguments_on_host():
+    """kernel_params beta: one value, or one per axis (sigpy's per-axis
+    param); a wrong count is a ValueError before any device work."""
+    import torch
+    from mr_recon_b200.interp import _beta
+    assert _beta(None, 2) == 1.0
+    assert _beta({"beta": 7.5}, 3) == 7.5
+    assert _beta({"beta": (7.5, 7.5)}, 2) == 7.5           # equal betas collapse to one
+    assert _beta({"beta": (7.5, 6.0)}, 2) == (7.5, 6.0)
+    assert _beta({"beta": torch.tensor([7.5, 6.0, 5.0])}, 3) == (7.5, 6.0, 5.0)
+    with pytest.raises(ValueError):
+        _beta({"beta": (7.5, 6.0)}, 3)
+
+
+def test_type3_checks_bases_before_device_work():
+    """type3_nufft takes 1-3 bases (the tile kernels' dimensions) and says so
+    for more, as NotImplementedError, before any CUDA call."""
+    import torch
+    from mr_recon_b200.linops import type3_nufft
+    with pytest.raises(NotImplementedError):
+        type3_nufft(torch.zeros(4, 6, 6), torch.zeros(4, 10))
+    with pytest.raises(AssertionError):
+        type3_nufft(torch.zeros(2, 6, 6), torch.zeros(3, 10))
