@@ -42,11 +42,35 @@ NCOIL = 32
 NINTL, NSAMP = 48, 2048
 OS, W = 1.25, 6
 WORKLOAD = "2D multi-coil KB NUFFT fwd+adj: 256x256 c64, 32 coils, VD spiral 48x2048, os 1.25, W 6"
-# DRAM bytes (read + write) per launch of each tile kernel on this workload,
-# from one ncu capture (profiles/grid_interp_kernels_spiral256_c32.md).
 HOST_AHEAD_S = 0.4e-3  # device-side wait before each timed step: longer than the host's enqueue of one step
+# DRAM bytes (read + write) per launch of each tile kernel on this workload,
+# from one ncu capture of the kernels named in TRAFFIC_SOURCE (ncu cannot run
+# inside the timed program, so the figure is carried here and labelled).
 GRID_TRAFFIC_BYTES = 33_565_440 + 60_928
 INTERP_TRAFFIC_BYTES = 26_191_360 + 1_033_728
+TRAFFIC_SOURCE = ("ncu --set full capture of k_grid_reg<6,1> and k_interp_reg<2,7,1> on this workload "
+                  "(dram__bytes_read.sum + dram__bytes_write.sum per launch)")
+CG_FIXTURE = os.path.join(ROOT, "tests", "golden", "cg_config2.npz")
+# Speed of the oracle port relative to the reference's own CPU path
+# (triton_nufft on CPU tensors, its torch fallback) on this workload: both
+# timed on the same 8 host threads of the development machine, 8 coils,
+# forward + adjoint (the reference cannot run where the benchmark runs).
+PORT_VS_REFERENCE = {"port_msample_coil_s": 0.40, "reference_msample_coil_s": 0.94, "threads": 8,
+                     "ratio": 0.43}
+
+
+def host_info():
+    """Host CPU model and logical core count (for the CPU baselines)."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu_model": model, "host_logical_cores": os.cpu_count()}
 
 
 def load_peaks():
@@ -118,9 +142,11 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_baseline(trj, imgs, coils, repeats=1):
+def cpu_baseline(trj, imgs, coils, repeats=1, outputs=None):
     """The CPU oracle (a numpy restatement of the reference's CPU path) on
-    `coils` coils, one coil per thread. Returns (Msample*coil/s, threads, seconds)."""
+    `coils` coils, one coil per thread. Returns (Msample*coil/s, threads,
+    seconds); with `outputs` (a dict) also stores the last repeat's forward
+    k-space ("ksp", (1, coils, ...)) and adjoint images ("img")."""
     from concurrent.futures import ThreadPoolExecutor
     from oracle import nufft_oracle as O
     O.FFT_WORKERS = 1
@@ -132,8 +158,11 @@ def cpu_baseline(trj, imgs, coils, repeats=1):
         for _ in range(repeats):
             t0 = time.perf_counter()
             ks = list(ex.map(lambda c: nf.forward(imgs[:, c:c + 1], trj), range(coils)))
-            list(ex.map(lambda c: nf.adjoint(ks[c], trj), range(coils)))
+            bs = list(ex.map(lambda c: nf.adjoint(ks[c], trj), range(coils)))
             t_total += time.perf_counter() - t0
+    if outputs is not None:
+        outputs["ksp"] = np.concatenate(ks, 1)
+        outputs["img"] = np.concatenate(bs, 1)
     return coils * M * repeats / t_total / 1e6, threads, t_total
 
 
@@ -401,20 +430,21 @@ def run_reference(args, rank):
         return
     _, _, imgs, trj = make_inputs(0)
     ncores = os.cpu_count() or 1
-    per = max(1, args.steps + args.warmup)
-    coils = int(max(1, min(ncores, 8, 160 // per)))
+    # one coil per host thread, every thread busy, at most the 32 coils of the workload
+    coils = int(max(1, min(ncores, NCOIL)))
     for _ in range(min(args.warmup, 1)):
         cpu_baseline(trj, imgs, coils, 1)
     v, thr, secs = cpu_baseline(trj, imgs, coils, args.steps)
     M = NINTL * NSAMP
     ms = secs / args.steps * 1e3
+    sample = f"{coils} of 32 coils per step (one per host thread), full 98304-sample spiral, fwd+adj"
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "complex64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "sample_coils_per_step": coils, "samples_per_coil": M},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": thr, "kind": "port",
-                         "sample": f"{coils} of 32 coils per step, full 98304-sample spiral, fwd+adj"},
+        "cpu_baseline": dict({"value": v, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample,
+                              "port_vs_reference_cpu": PORT_VS_REFERENCE}, **host_info()),
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -430,7 +460,9 @@ def main():
     ap.add_argument("--no-cg", action="store_true")
     ap.add_argument("--c3-n", type=int, default=192, help="c3 image edge (192 = the configuration)")
     ap.add_argument("--c3-spokes", type=int, default=20000, help="c3 kooshball spokes (20000 = the configuration)")
-    ap.add_argument("--extra", default="", help="comma list of extra workloads: c3 (3D), c4 (batched CG), c5 (B0 segments)")
+    ap.add_argument("--extra", default="c3,c4,c5",
+                    help="comma list of the other configurations to add to the line: c3 (3D), c4 (batched "
+                         "uneven CG), c5 (B0 segments); empty for none")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -515,6 +547,7 @@ def main():
     achieved = alg / (dms / 1e3) / 1e9
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                "traffic_source": TRAFFIC_SOURCE,
                 "algorithmic_bytes": alg, "kernel_ms": dms,
                 "stage_ms_per_step": {k: v[0] / args.steps for k, v in stage.items() if v[1]},
                 "host_enqueue_ms_per_step": host_s * 1e3 / args.steps}
@@ -580,8 +613,7 @@ def main():
         return world * C * M * ne / (t / 1e3) / 1e6
 
     e2e_val = time_e2e(e2e_step)
-    # against the device-resident run: the forward is bit-identical, the adjoint
-    # differs in rounding only (split tiles sum their halves with atomics)
+    # against the device-resident run (the same kernels: bit-identical)
     def _rel(a, b):
         return float((a - b).abs().square().sum().sqrt() / b.abs().square().sum().sqrt())
     match = max(_rel(out_h, back.cpu()), _rel(ksp_h, ksp.cpu()))
@@ -600,13 +632,19 @@ def main():
         A = sense_linop(trj[0], torch.from_numpy(mps_np).to(dev), nufft=nf)
         kk = A.forward(torch.from_numpy(x_np).to(dev))
         kk = torch.from_numpy(synth.add_noise(kk.cpu().numpy(), 30.0, rng)).to(dev)
-        max_eig = 1.0
-        for _ in range(15):  # power method (setup, not timed)
-            v = torch.randn(IM, dtype=torch.complex64, device=dev) if _ == 0 else v
-            z = A.normal(v)
-            max_eig = float(torch.linalg.vector_norm(z))
-            v = z / max_eig
-        max_eig *= 1.01
+        # the oracle's float64 CG on this problem (rank 0's inputs), computed
+        # on the CPU by tests/golden/make_cg_config2.py with its max eigenvalue
+        fix = np.load(CG_FIXTURE) if (rank == 0 and os.path.exists(CG_FIXTURE)) else None
+        if fix is not None:
+            max_eig = float(fix["max_eigen"])
+        else:
+            max_eig = 1.0
+            for _ in range(15):  # power method (setup, not timed)
+                v = torch.randn(IM, dtype=torch.complex64, device=dev) if _ == 0 else v
+                z = A.normal(v)
+                max_eig = float(torch.linalg.vector_norm(z))
+                v = z / max_eig
+            max_eig *= 1.01
         solver = SenseCG(A.plan, A.mps, A.dcf, 20, 1e-3, max_eig)
         solver.ksp.copy_(kk.reshape(-1))
         x_eager = solver.solve().clone()
@@ -630,14 +668,34 @@ def main():
         e_ms = c0.elapsed_time(c1) / 5
         cg = {"solves_per_s_graph": world * 1e3 / g_ms, "solves_per_s_eager": world * 1e3 / e_ms,
               "ms_per_solve_graph": g_ms, "iterations": 20, "lambda": 1e-3,
-              "graph_vs_eager_rel_diff": float((x_graph - x_eager).norm() / x_eager.norm())}
+              "graph_vs_eager_rel_diff": float((x_graph - x_eager).norm() / x_eager.norm()),
+              "precision": "complex128 iterates, complex64 NUFFT, float64 fixed-order sums"}
+        if fix is not None:
+            ref = torch.from_numpy(fix["x_cg64"]).to(dev).reshape(-1)
+            cg["rel_err_vs_oracle_cg64"] = float((x_graph.reshape(-1) - ref).norm() / ref.norm())
+            cg["reference_f32_arith_rel_err_vs_oracle_cg64"] = float(fix["rel_f32_arith"])
 
     cpu = None
+    rel_err = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, thr, secs = cpu_baseline(trj_np, imgs_np, 8, 2)
-        cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port",
-               "sample": "8 of 32 coils (one per thread), full 98304-sample spiral, fwd+adj, 2 repeats",
-               "seconds": secs}
+        nb = int(min(NCOIL, max(1, os.cpu_count() or 1)))
+        outs = {}
+        v, thr, secs = cpu_baseline(trj_np, imgs_np, nb, 2, outputs=outs)
+        cpu = dict({"value": v, "unit": UNIT, "cores": thr, "kind": "port",
+                    "sample": f"{nb} of 32 coils (one per host thread), full 98304-sample spiral, fwd+adj, "
+                              "2 repeats", "seconds": secs, "port_vs_reference_cpu": PORT_VS_REFERENCE},
+                   **host_info())
+        # the GPU results against the oracle's on the same coils and inputs
+        k_o = torch.from_numpy(outs["ksp"]).to(dev)
+        b_g = nf.adjoint(k_o, trj)
+
+        def _r(a, b):
+            return float((a - b).abs().square().sum().sqrt() / b.abs().square().sum().sqrt())
+        rel_err = {"forward": _r(ksp[:, :nb], k_o),
+                   "adjoint": _r(b_g, torch.from_numpy(outs["img"]).to(dev)),
+                   "against": f"CPU oracle, {nb} coils, same inputs"}
+        if cg is not None and "rel_err_vs_oracle_cg64" in cg:
+            rel_err["cg_sense"] = cg["rel_err_vs_oracle_cg64"]
 
     extra = {}
     if rank == 0 and world == 1:
@@ -660,7 +718,7 @@ def main():
                        "host_ahead": f"{HOST_AHEAD_S * 1e3:.1f} ms device-side wait before each timed step "
                                      "(outside the events) while the host enqueues it",
                        "parallelism": f"replicas x{world}", "plan": stats},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "cg_sense": cg,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "cg_sense": cg, "rel_err": rel_err,
             "gpu_launches": launches_per_step * args.steps, "clocks": clocks,
         }
         line.update(extra)

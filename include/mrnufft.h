@@ -80,8 +80,9 @@ int mrn_plan_offsets(const mrn_plan* plan, int64_t* img_off, int64_t* ksp_off,
 /* Totals: [0] image elems, [1] ksp elems, [2] grid elems, [3] trj floats,
  * [4] number of tiles, [5] oversampled size dim0, [6] dim1, [7] dim2 (slice 0). */
 int mrn_plan_sizes(const mrn_plan* plan, int64_t* out8);
-/* Host-side, after a synchronize: number of interp and gridding work items,
- * gridding entries, and split (multi-item) gridding tiles, in out4. */
+/* Number of interp and gridding work items, gridding entries, and split
+ * (multi-item) gridding tiles of the bound trajectory, in out4 (all zero
+ * before mrn_plan_set_traj). Synchronises the plan's device to read them. */
 int mrn_plan_stats(mrn_plan* plan, int64_t* out4);
 
 /* Plan options (no counterpart in the reference).
@@ -91,7 +92,9 @@ int mrn_plan_stats(mrn_plan* plan, int64_t* out4);
 #define MRN_OPT_FAST_KERNELS 1
 /* MRN_OPT_WARP_GRIDDING (default 1): 2D gridding with one warp per output tile
  * (no atomics, reproducible summation order) where the fast kernels apply; 0
- * uses the shared-memory-atomic tile kernel. */
+ * uses the shared-memory-atomic tile kernel (whose shared-memory float atomics
+ * add in a run-dependent order). On every path, tiles split over several
+ * work items are combined by adding their partial tiles in item order. */
 #define MRN_OPT_WARP_GRIDDING 2
 /* MRN_OPT_WEIGHT_TABLES (default 0): in 2D, mrn_plan_set_traj evaluates the KB
  * weights of every sample once and stores them (~80 bytes per sample and per
@@ -110,7 +113,7 @@ int mrn_plan_stats(mrn_plan* plan, int64_t* out4);
 #define MRN_OPT_GRID_TILE 7
 /* MRN_OPT_REG_GRIDDING (default 1): 2D gridding tiles of at most 8x8 cells
  * keep their accumulator in registers (two warps per tile, lane = coil);
- * 0 keeps it in shared memory. Both sum in the same fixed order. */
+ * 0 keeps it in shared memory. Each gives the same bits from run to run. */
 #define MRN_OPT_REG_GRIDDING 8
 /* MRN_OPT_REG_INTERP (default 1): 2D and 3D interpolation with one lane per
  * coil over the tile region staged as [cell][coil] (packed two-lane FMAs); 0
@@ -140,8 +143,15 @@ int mrn_plan_timing(mrn_plan* plan, double* ms8, int64_t* count8);
  * Bind a trajectory (device, float32, all slices back to back). Scales it
  * (triton_nufft._scale_trj, fourier.py:420-430), wraps it circularly
  * (torch.remainder, ungrid.py:873), and sorts the samples into spatial tiles
- * for both interpolation and gridding. Asynchronous; safe to capture in a
- * CUDA graph. Must be called again when the trajectory values change.
+ * for both interpolation and gridding. Must be called again when the
+ * trajectory values change. NOT asynchronous and not for use under stream
+ * capture: it waits for the stream once, to read back the number of gridding
+ * entries, and may allocate device memory when that number (or the work-item
+ * or partial-tile capacity derived from it) outgrows the plan's buffers.
+ * Everything else (sorts, work items, their longest-first order) stays on the
+ * device. Plans are limited to fewer than 2^31 samples and 2^31 gridding
+ * entries (2^d entries per sample at most): mrn_plan_create returns
+ * MRN_ERR_UNSUPPORTED beyond that.
  */
 int mrn_plan_set_traj(mrn_plan* plan, const float* trj, void* stream);
 
@@ -194,27 +204,34 @@ int mrn_sense_normal(mrn_plan* plan, const void* x, const void* mps, const float
 
 /*
  * Conjugate-gradient vector steps for n_slices independent systems (the loop
- * body of conjugate_gradient, algs.py:779-872), complex64 vectors with
- * float64 dot products and norms; per-slice scalars stay on the device, so a
- * whole solve can be captured in a CUDA graph. Vectors use the per-slice
- * image layout (one image per slice). state: float64 [n_slices * 8] owned by
- * the caller:
+ * body of conjugate_gradient, algs.py:779-872). The iterates x, r, p are
+ * complex128 (per-slice image layout, one image per slice); the operator
+ * works on a complex64 copy p32 of p that these calls keep current, and its
+ * result Ap is complex64. Dot products and norms are float64 sums in a fixed
+ * order; per-slice scalars stay on the device, so a whole solve can be
+ * captured in a CUDA graph and replays to the same bits as the eager solve.
+ * (The reference runs CG in float32 vectors and dots; float64 iterates keep a
+ * 20-iteration solve within ~1e-4 of float64 CG although the NUFFT is
+ * complex64.) state: float64 [n_slices * 8] owned by the caller:
  *   [0] rz  [1] pAp (accumulated)  [2] rr (accumulated)  [3] done  [4] tol^2
  *   [5] iterations  [6] last alpha  [7] last beta
- * mrn_cg_init : zero state; r = b - Ab (Ab given), p = r, x = b, rz = |r|^2
- * per iteration: Ap = (A^H A + lam) p accumulating pAp into state[1]
- *                (mrn_sense_normal with pap = state + 1, pap_stride = 8), then
- * mrn_cg_step : alpha = rz/pAp; x += alpha p; r -= alpha Ap; rr = |r|^2
- * mrn_cg_dir  : done |= rr < tol^2; beta = rr/rz; p = r + beta p; rz = rr;
- *               pAp = rr = 0 for the next iteration
+ * mrn_cg_init : zero state; r = b - Ab (b, Ab complex64), p = r, x = b,
+ *               p32 = p, rz = |r|^2
+ * per iteration: Ap = (A^H A + lam) p32 accumulating Re<p32, Ap> into
+ *                state[1] (mrn_sense_normal with pap = state + 1,
+ *                pap_stride = 8), then
+ * mrn_cg_step : alpha = rz/pAp; x += alpha p; r -= alpha Ap; rr = |r|^2;
+ *               x32 = x (complex64) when x32 is not NULL
+ * mrn_cg_dir  : done |= rr < tol^2; beta = rr/rz; p = r + beta p; p32 = p;
+ *               rz = rr; pAp = rr = 0 for the next iteration
  * Once a slice is done its vectors are left unchanged (the reference breaks
  * out of the loop at the same point, algs.py:859-860).
  */
-int mrn_cg_init(mrn_plan* plan, const void* b, const void* Ab, void* x, void* r, void* p,
+int mrn_cg_init(mrn_plan* plan, const void* b, const void* Ab, void* x, void* r, void* p, void* p32,
                 double* state, double tol, void* stream);
-int mrn_cg_step(mrn_plan* plan, void* x, void* r, const void* p, const void* Ap,
+int mrn_cg_step(mrn_plan* plan, void* x, void* r, const void* p, const void* Ap, void* x32,
                 double* state, void* stream);
-int mrn_cg_dir(mrn_plan* plan, const void* r, void* p, double* state, void* stream);
+int mrn_cg_dir(mrn_plan* plan, const void* r, void* p, void* p32, double* state, void* stream);
 /* Per-slice Re<a, b> in float64, accumulated into out[slice] (caller zeroes). */
 int mrn_cg_dot(mrn_plan* plan, const void* a, const void* b, double* out, void* stream);
 

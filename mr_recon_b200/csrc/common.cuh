@@ -14,6 +14,7 @@ namespace mrn {
 constexpr int kMaxDim = 3;
 constexpr int kMaxTaps = 16;     // candidate taps per dim: floor(W) + 1 <= 16 -> W < 16
 constexpr int kThreads = 256;    // threads per CTA of the tile kernels
+constexpr int kMaxRedBlocks = 1024;  // CTAs per slice of the CG vector kernels
 constexpr int kWarps = kThreads / 32;
 
 // Geometry of one slice (one NUFFT problem) of a plan. Device-resident table.
@@ -44,15 +45,33 @@ struct SliceGeom {
   float inv_sqrt_n;      // 1 / sqrt(prod(n)) (fourier.py:462, 522)
 };
 
-// Work item: one tile (or a chunk of a heavy tile) of one slice.
+// Work item: one tile (or a chunk of a heavy tile) of one slice. Item lists
+// are launched at a capacity fixed when the trajectory is bound; entries past
+// the real items are padding with slice = -1, which the kernels skip.
 struct Item {
-  int slice;
+  int slice;     // -1: padding item, nothing to do
   int tile;      // tile id local to the slice
   int start;     // first entry in the sorted arrays
   int count;     // entries in this item
-  int split;     // 1 if the tile is shared by several items (gridding: atomic write-back)
+  int split;     // gridding: 0 if the item owns its tile, else 1 + its partial-tile slot
   int pad[3];
 };
+
+// Where the items of a split gridding tile (one whose entries were cut into
+// several items) put their partial tiles: slot s holds, for every coil, the
+// tile's cells in row-major order over the tile extent. A reduction pass then
+// adds the slots of each split tile in item order and stores the sum, so the
+// result does not depend on which item finishes first.
+struct SplitOut {
+  float2* part;         // [slot][coil][cell]
+  int64_t slot_stride;  // max_coil * cell_cap
+  int cell_cap;         // cells of the largest gridding tile
+  int pad;
+};
+
+__device__ __forceinline__ float2* split_slot(const SplitOut& so, int split, int coil, int cell) {
+  return so.part + (int64_t)(split - 1) * so.slot_stride + (int64_t)coil * so.cell_cap + cell;
+}
 
 constexpr int kKBTerms = 32;  // terms of the I0 power series kept in KBParams
 
@@ -204,6 +223,38 @@ __device__ __forceinline__ float kb_tap_du(float dx, float r, float beta) {
   return dkb * sgn / r;
 }
 
+// ---------------------------------------------------------------------------
+// Run-to-run reproducible float64 reductions. Float atomics add in whatever
+// order the blocks arrive; these helpers instead have every block store its
+// partial sum, and the last block to finish (found with an integer counter)
+// adds the partials in a fixed order.
+// ---------------------------------------------------------------------------
+
+// Call in every thread of the block after thread 0 has stored the block's
+// partial sum(s) to global memory. True in every thread of the last block of
+// the grid to arrive; that block then sees every other block's partials (read
+// them with __ldcg) and must reset *counter to 0 before it exits.
+__device__ __forceinline__ bool arrive_last_block(unsigned* counter, unsigned nblocks) {
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(counter, 1u) == nblocks - 1u;
+  }
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
+}
+
+// Sum of src[0..n) by one warp in a fixed order: lane-strided partial sums,
+// then a butterfly of shuffles. Lane 0's result is the same on every run.
+__device__ __forceinline__ double warp_sum_fixed(const double* src, int64_t n, int lane) {
+  double a = 0.0;
+  for (int64_t i = lane; i < n; i += 32) a += __ldcg(src + i);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  return a;
+}
+
 // torch.remainder for float32 by a positive modulus (ungrid.py:873).
 __device__ __forceinline__ float remainder_f32(float a, float n) {
   float m = fmodf(a, n);
@@ -257,9 +308,14 @@ struct mrn_plan {
   int tmax_cells[mrn::kMaxDim] = {1, 1, 1};   // largest interpolation tile extent per dim
   int tmax_gcells[mrn::kMaxDim] = {1, 1, 1};  // largest gridding tile extent per dim
   int64_t n_entries_grid = 0;  // gridding entries of the bound trajectory
+  // Launch extents of the bound trajectory: upper bounds of the interpolation
+  // items, gridding items and split gridding tiles (the exact counts stay on
+  // the device in d_counts; mrn_plan_stats reads them).
   int64_t n_items_interp = 0, n_items_grid = 0, n_split = 0;
   int64_t cap_entries = 0, cap_items_i = 0, cap_items_g = 0;  // allocated capacities
   int64_t cap_tiles = 0;
+  int64_t cap_part = 0;        // complex elements allocated in d_part
+  int64_t cap_sort = 0;        // entries of the item-ordering sort buffers
   bool traj_set = false;
 
   // device buffers
@@ -298,12 +354,19 @@ struct mrn_plan {
   mrn::Item* d_items_i = nullptr;
   mrn::Item* d_items_g = nullptr;
   int* d_counts = nullptr;          // [0] n_items_i [1] n_items_g [2] n_entries_g [3] n_split
-  int* d_split_tiles = nullptr;     // global tile ids of split gridding tiles
+                                    // [4] partial-tile slots in use
+  int4* d_split_tiles = nullptr;    // split gridding tiles: {global tile, first slot, items, 0}
+  float2* d_part = nullptr;         // partial tiles of split gridding tiles (SplitOut)
+  mrn::Item* d_items_tmp = nullptr; // items before the longest-first ordering
+  unsigned* d_sort_key[2] = {nullptr, nullptr};  // item ordering: keys in / out
+  int* d_sort_idx[2] = {nullptr, nullptr};       // item ordering: indices in / out
   void* d_cub_tmp = nullptr;
   size_t cub_tmp_bytes = 0;
   float2* d_grid = nullptr;         // internal oversampled grid (natural order, grouped)
   float2* d_ksp_tmp = nullptr;      // sample scratch for normal operators
-  unsigned* d_sync = nullptr;       // last-block counters
+  unsigned* d_sync = nullptr;       // last-block counters: [0] k_cg_dir, [1] CG sums, [2] k_post
+  double* d_red = nullptr;          // CG block partial sums, [n_slices][kMaxRedBlocks]
+  double* d_rowpart = nullptr;      // k_post per-row partials of Re<x, out>, [n_xrow]
   // FFT groups: slices with identical Nos share one batched cuFFT plan
   struct FftGroup {
     int nos[mrn::kMaxDim];

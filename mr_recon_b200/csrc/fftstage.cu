@@ -94,16 +94,45 @@ k_pre(const SliceGeom* __restrict__ sl, int ns, const float* __restrict__ apod,
 // One warp per image row. Plain: rows over (slice, coil, outer image index),
 // out[c][q] = Y_c[(q - N//2) mod Nos] * apod(q) * scale.
 // Sense: rows over (slice, outer image index), out[q] = scale * apod(q) *
-// sum_c conj(mps_c[q]) Y_c[...] (+ lam * xin[q]); pap[slice] += Re<xin, out>.
+// sum_c conj(mps_c[q]) Y_c[...] (+ lam * xin[q]); pap[slice] += Re<xin, out>,
+// summed reproducibly: each row's warp stores its partial in rowpart[row] and
+// the last block adds every slice's rows in row order.
+template <int D>
+__device__ __forceinline__ void post_row(const SliceGeom* __restrict__ sl, int ns, const float* __restrict__ apod,
+                                         const float2* __restrict__ grid, const float2* __restrict__ mps,
+                                         int mode, float scale, float2* __restrict__ out,
+                                         const float2* __restrict__ xin, float lam,
+                                         double* __restrict__ rowpart, int64_t row, int lane);
+
 template <int D>
 __global__ void __launch_bounds__(256)
 k_post(const SliceGeom* __restrict__ sl, int ns, const float* __restrict__ apod,
        const float2* __restrict__ grid, const float2* __restrict__ mps, int mode, float scale,
        float2* __restrict__ out, const float2* __restrict__ xin, float lam, double* __restrict__ pap,
-       int pap_stride, int64_t nrows) {
+       int pap_stride, int64_t nrows, double* __restrict__ rowpart, unsigned* __restrict__ counter) {
   const int64_t row = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  if (row >= nrows) return;
+  if (row < nrows)
+    post_row<D>(sl, ns, apod, grid, mps, mode, scale, out, xin, lam, pap ? rowpart : nullptr, row, lane);
+  if (!pap) return;
+  __syncthreads();  // this block's row partials are stored before thread 0 arrives
+  if (!arrive_last_block(counter, gridDim.x)) return;
+  const int warp = threadIdx.x >> 5;
+  for (int q = warp; q < ns; q += 8) {
+    const SliceGeom& g = sl[q];
+    const double v = warp_sum_fixed(rowpart + g.xrow_off, g.nimg / g.n[D - 1], lane);
+    if (lane == 0) pap[(int64_t)q * pap_stride] += v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *counter = 0u;
+}
+
+template <int D>
+__device__ __forceinline__ void post_row(const SliceGeom* __restrict__ sl, int ns, const float* __restrict__ apod,
+                                         const float2* __restrict__ grid, const float2* __restrict__ mps,
+                                         int mode, float scale, float2* __restrict__ out,
+                                         const float2* __restrict__ xin, float lam,
+                                         double* __restrict__ rowpart, int64_t row, int lane) {
   const int s = slice_by_row(sl, ns, row, mode == kPostSense ? 2 : 1);
   const SliceGeom& g = sl[s];
   const int64_t r = row - (mode == kPostSense ? g.xrow_off : g.irow_off);
@@ -165,9 +194,9 @@ k_post(const SliceGeom* __restrict__ sl, int ns, const float* __restrict__ apod,
       }
       orow_p[j] = v;
     }
-    if (pap) {
+    if (rowpart) {
       for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
-      if (lane == 0) atomicAdd(pap + (int64_t)s * pap_stride, part);
+      if (lane == 0) rowpart[row] = part;
     }
   }
 }
@@ -222,14 +251,15 @@ int launch_pre(mrn_plan* P, PreMode mode, const float2* src, const float2* mps, 
 int launch_post(mrn_plan* P, PostMode mode, const float2* mps, float2* out, float scale,
                 const float2* xin, float lam, double* pap, int pap_stride, cudaStream_t st) {
   const int64_t nrows = mode == kPostSense ? P->n_xrow : P->n_irow;
+  if (mode != kPostSense) pap = nullptr;  // Re<x, out> exists only for the SENSE form
   const unsigned blocks = (unsigned)((nrows + 7) / 8);
   if (blocks == 0) return MRN_OK;
   if (P->ndim == 1)
-    k_post<1><<<blocks, 256, 0, st>>>(P->d_slices, P->nslices, P->d_apod, P->d_grid, mps, mode, scale, out, xin, lam, pap, pap_stride, nrows);
+    k_post<1><<<blocks, 256, 0, st>>>(P->d_slices, P->nslices, P->d_apod, P->d_grid, mps, mode, scale, out, xin, lam, pap, pap_stride, nrows, P->d_rowpart, P->d_sync + 2);
   else if (P->ndim == 2)
-    k_post<2><<<blocks, 256, 0, st>>>(P->d_slices, P->nslices, P->d_apod, P->d_grid, mps, mode, scale, out, xin, lam, pap, pap_stride, nrows);
+    k_post<2><<<blocks, 256, 0, st>>>(P->d_slices, P->nslices, P->d_apod, P->d_grid, mps, mode, scale, out, xin, lam, pap, pap_stride, nrows, P->d_rowpart, P->d_sync + 2);
   else
-    k_post<3><<<blocks, 256, 0, st>>>(P->d_slices, P->nslices, P->d_apod, P->d_grid, mps, mode, scale, out, xin, lam, pap, pap_stride, nrows);
+    k_post<3><<<blocks, 256, 0, st>>>(P->d_slices, P->nslices, P->d_apod, P->d_grid, mps, mode, scale, out, xin, lam, pap, pap_stride, nrows, P->d_rowpart, P->d_sync + 2);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? MRN_OK : cuda_fail(e);
 }

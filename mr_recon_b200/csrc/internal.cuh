@@ -21,6 +21,23 @@ inline int set_dynamic_smem(Kern kernel, size_t dyn) {
 // Which grid layout a tile kernel reads or writes.
 enum GridLayout { kInternal = 0, kUser = 1 };
 
+// Cells of the largest gridding tile of the plan (the partial-tile slot size per coil).
+inline int grid_tile_cells(const mrn_plan* P) {
+  int c = 1;
+  for (int i = 0; i < P->ndim; ++i) c *= P->tmax_gcells[i];
+  return c;
+}
+
+// Partial-tile slots of split gridding tiles, as the gridding kernels take them.
+inline SplitOut split_out(const mrn_plan* P) {
+  SplitOut so;
+  so.part = P->d_part;
+  so.cell_cap = grid_tile_cells(P);
+  so.slot_stride = (int64_t)P->max_coil * so.cell_cap;
+  so.pad = 0;
+  return so;
+}
+
 // Tile kernels (tiles.cu)
 int launch_interp(mrn_plan* P, const float2* grid, GridLayout layout, float2* ksp, float scale,
                   const float2* temporal, cudaStream_t st);

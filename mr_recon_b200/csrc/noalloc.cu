@@ -160,7 +160,10 @@ extern "C" int mrn_interp_noalloc(int ndim, const int* grid_size, int n_coil, in
     g.ntaps[i] = (int)floor(width[i]) + 1;
     g.K = g.ntaps[i] > g.K ? g.ntaps[i] : g.K;
   }
-  // scratch layout: [lo: n_pts*d int32][weights: n_pts*d*K float32], 256-B aligned
+  // scratch layout: [lo: n_pts*d int32][weights: n_pts*d*K float32], 256-B aligned.
+  // The sample count is bounded first, so the byte counts below cannot wrap.
+  if ((uint64_t)n_pts > (uint64_t)(kNoAllocScratchBytes / ((size_t)ndim * (1 + g.K) * sizeof(float))))
+    return MRN_ERR_SCRATCH;
   const size_t lo_bytes = (((size_t)n_pts * ndim * sizeof(int)) + 255) & ~(size_t)255;
   const size_t need = lo_bytes + (size_t)n_pts * ndim * g.K * sizeof(float);
   if (need > kNoAllocScratchBytes) return MRN_ERR_SCRATCH;
@@ -174,7 +177,8 @@ extern "C" int mrn_interp_noalloc(int ndim, const int* grid_size, int n_coil, in
   cudaStream_t st = (cudaStream_t)stream;
   const unsigned b1 = (unsigned)((n_pts + 255) / 256);
   k_na_weights<<<b1, 256, 0, st>>>(g, locs, n_pts, lo, w);
-  const int64_t work = n_pts * n_coil;
+  const int64_t work = n_pts * n_coil;  // n_pts < 2^23 here, so no overflow
+  if ((work + 255) / 256 > (int64_t)INT32_MAX) return MRN_ERR_ARG;
   const unsigned b2 = (unsigned)((work + 255) / 256);
   k_na_gather<<<b2, 256, 0, st>>>(g, n_coil, n_pts, lo, w, (const float2*)grid, (float2*)out);
   cudaError_t e = cudaGetLastError();

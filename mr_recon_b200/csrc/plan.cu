@@ -181,31 +181,57 @@ __global__ void k_item_counts(const int* __restrict__ start, const int* __restri
   nitems[t] = max(min_items, (c + chunk - 1) / chunk);
 }
 
+// Work items of every tile at the scanned offsets. Gridding tiles with more
+// than one item are split tiles: each gets a run of n partial-tile slots
+// (counts[4] hands them out) and a record {tile, first slot, n} in
+// split_tiles (counts[3] counts them); item q of the tile writes slot
+// first + q. The order in which tiles claim slots does not matter: the
+// reduction adds a tile's slots in item order.
 __global__ void k_emit_items(const SliceGeom* __restrict__ sl, int ns, const int* __restrict__ start,
                              const int* __restrict__ end, const int* __restrict__ nitems,
                              const int* __restrict__ ioff, int ntiles, int chunk,
-                             Item* __restrict__ items, int* __restrict__ split_tiles,
-                             int* __restrict__ counts, int count_slot, int split_slot, int gridding) {
+                             Item* __restrict__ items, int4* __restrict__ split_tiles,
+                             int* __restrict__ counts, int count_slot, int gridding) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ntiles) return;
   const int n = nitems[t];
   const int s = find_slice_by_tile(sl, ns, t, gridding);
   const int c = end[t] - start[t];
+  int base = -1;
+  if (gridding && n > 1) {
+    base = atomicAdd(&counts[4], n);
+    const int k = atomicAdd(&counts[3], 1);
+    split_tiles[k] = make_int4(t, base, n, 0);
+  }
   for (int q = 0; q < n; ++q) {
     Item it;
     it.slice = s;
     it.tile = t - (gridding ? sl[s].gtile_base : sl[s].tile_base);
     it.start = start[t] + q * chunk;
     it.count = max(0, min(chunk, c - q * chunk));
-    it.split = n > 1 ? 1 : 0;
+    it.split = base >= 0 ? base + q + 1 : 0;
     it.pad[0] = it.pad[1] = it.pad[2] = 0;
     items[ioff[t] + q] = it;
   }
   if (t == ntiles - 1) counts[count_slot] = ioff[t] + n;
-  if (split_slot >= 0 && n > 1) {
-    const int k = atomicAdd(&counts[split_slot], 1);
-    split_tiles[k] = t;
-  }
+}
+
+// Sort keys of the longest-first item order: count + 1 for real items, 0 for
+// the padding (slice -1) past them, so a stable descending sort keeps real
+// items of equal length in tile order and leaves the padding last.
+__global__ void k_item_keys(const Item* __restrict__ items, int64_t n, unsigned* __restrict__ key,
+                            int* __restrict__ idx) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Item it = items[i];
+  key[i] = it.slice < 0 ? 0u : (unsigned)it.count + 1u;
+  idx[i] = (int)i;
+}
+
+__global__ void k_gather_items(const Item* __restrict__ src, const int* __restrict__ idx, int64_t n,
+                               Item* __restrict__ dst) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[idx[i]];
 }
 
 __global__ void k_total(const int* __restrict__ off, const int* __restrict__ cnt, int64_t n,
@@ -224,18 +250,6 @@ static int tiles_for(int nos, int edge, int K) {
   return std::max(1, nt);
 }
 
-// Reorder work items by decreasing entry count (stable), on the host.
-static int sort_items_longest_first(Item* d_items, int64_t n, cudaStream_t st) {
-  if (n <= 1) return MRN_OK;
-  std::vector<Item> h((size_t)n);
-  cudaError_t e = cudaMemcpyAsync(h.data(), d_items, (size_t)n * sizeof(Item), cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return cuda_fail(e);
-  std::stable_sort(h.begin(), h.end(), [](const Item& a, const Item& b) { return a.count > b.count; });
-  e = cudaMemcpyAsync(d_items, h.data(), (size_t)n * sizeof(Item), cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  return e == cudaSuccess ? MRN_OK : cuda_fail(e);
-}
 
 // Tile arrays are allocated for the larger of the two tilings.
 // Kernel shape parameters: beta per dimension, and the I0 power series
@@ -347,12 +361,16 @@ static int retile(mrn_plan* P) {
   int rc = MRN_OK;
   if (need > P->cap_tiles) {
     int** bufs[] = {&P->d_tile_start_i, &P->d_tile_end_i, &P->d_tile_start_g, &P->d_tile_end_g,
-                    &P->d_tile_nitems, &P->d_tile_item_off, &P->d_split_tiles};
+                    &P->d_tile_nitems, &P->d_tile_item_off};
     for (int** b : bufs)
       if ((rc = dev_alloc(b, (size_t)need)) != MRN_OK) {
         P->cap_tiles = 0;
         return rc;
       }
+    if ((rc = dev_alloc(&P->d_split_tiles, (size_t)need)) != MRN_OK) {
+      P->cap_tiles = 0;
+      return rc;
+    }
     P->cap_tiles = need;
   }
   cudaError_t e = cudaSetDevice(P->device);
@@ -637,6 +655,8 @@ int mrn_plan_create(mrn_plan** out, int ndim, int n_slices, const int* im_size,
   PK(dev_alloc(&P->d_counts, 8));
   PK(dev_alloc(&P->d_sync, 64));
   CK(cudaMemset(P->d_sync, 0, 64 * sizeof(unsigned)));
+  PK(dev_alloc(&P->d_red, (size_t)n_slices * kMaxRedBlocks));
+  PK(dev_alloc(&P->d_rowpart, (size_t)std::max<int64_t>(P->n_xrow, 1)));
   if (!raw) {
     PK(dev_alloc(&P->d_grid, std::max<int64_t>(P->n_grid, 1)));
     PK(dev_alloc(&P->d_ksp_tmp, std::max<int64_t>(P->n_ksp, 1)));
@@ -724,7 +744,8 @@ int mrn_plan_destroy(mrn_plan* P) {
                   P->d_tile_end_g, P->d_tile_nitems, P->d_tile_item_off, P->d_items_i,
                   P->d_items_g, P->d_counts, P->d_split_tiles, P->d_cub_tmp, P->d_grid,
                   P->d_ksp_tmp, P->d_sync, P->d_wmeta_i, P->d_wtab_i, P->d_wmeta_g,
-                  P->d_wtab_g};
+                  P->d_wtab_g, P->d_part, P->d_items_tmp, P->d_sort_key[0], P->d_sort_key[1],
+                  P->d_sort_idx[0], P->d_sort_idx[1], P->d_red, P->d_rowpart};
   for (void* b : bufs)
     if (b) cudaFree(b);
   delete P;
@@ -753,7 +774,14 @@ int mrn_plan_sizes(const mrn_plan* P, int64_t* o) {
 
 int mrn_plan_stats(mrn_plan* P, int64_t* o) {
   if (!P || !o) return MRN_ERR_ARG;
-  o[0] = P->n_items_interp; o[1] = P->n_items_grid; o[2] = P->n_entries_grid; o[3] = P->n_split;
+  int hc[4] = {0, 0, 0, 0};
+  if (P->traj_set) {
+    cudaError_t e = cudaSetDevice(P->device);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(hc, P->d_counts, 4 * sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e);
+  }
+  o[0] = hc[0]; o[1] = hc[1]; o[2] = P->n_entries_grid; o[3] = hc[3];
   return MRN_OK;
 }
 
@@ -832,7 +860,7 @@ int mrn_plan_set_traj(mrn_plan* P, const float* trj, void* stream_) {
     CK(cudaGetLastError());
   }
 
-  // 4. per-tile ranges and work items
+  // 4. per-tile ranges
   CK(cudaMemsetAsync(P->d_tile_start_i, 0, T * sizeof(int), st));
   CK(cudaMemsetAsync(P->d_tile_end_i, 0, T * sizeof(int), st));
   CK(cudaMemsetAsync(P->d_tile_start_g, 0, TG * sizeof(int), st));
@@ -845,10 +873,20 @@ int mrn_plan_set_traj(mrn_plan* P, const float* trj, void* stream_) {
       k_tile_ranges<<<blocks_for(E), 256, 0, st>>>(P->d_key_g, E, TG, P->d_tile_start_g,
                                                    P->d_tile_end_g);
   }
+
+  // 5. work items, launched at capacities known from T, M and E alone, so the
+  // host needs no further read-back: a tile with c entries makes
+  // ceil(c / chunk) items (gridding: at least one), hence at most
+  // T + M / chunk + 1 of them; split gridding tiles have more than gchunk
+  // entries each (at most E / gchunk + 1 tiles) and ceil(c / gchunk) < 2 c / gchunk
+  // items each (fewer than 2 E / gchunk slots).
   const int chunk = P->max_chunk;
   const int gchunk = P->grid_chunk;
-  const int64_t max_items_i = (int64_t)T + M / chunk + 1;
+  const int64_t max_items_i = M > 0 ? (int64_t)T + M / chunk + 1 : 0;
   const int64_t max_items_g = (int64_t)TG + E / gchunk + 1;
+  const int64_t max_split = E > gchunk ? std::min<int64_t>(TG, E / gchunk + 1) : 0;
+  const int64_t max_slots = max_split > 0 ? 2 * (E / gchunk) + 1 : 0;
+  if (max_items_i >= (int64_t)INT32_MAX || max_items_g >= (int64_t)INT32_MAX) return MRN_ERR_UNSUPPORTED;
   if (P->cap_items_i < max_items_i) {
     RK(dev_alloc(&P->d_items_i, (size_t)max_items_i));
     P->cap_items_i = max_items_i;
@@ -857,34 +895,60 @@ int mrn_plan_set_traj(mrn_plan* P, const float* trj, void* stream_) {
     RK(dev_alloc(&P->d_items_g, (size_t)max_items_g));
     P->cap_items_g = max_items_g;
   }
-  k_item_counts<<<blocks_for(T), 256, 0, st>>>(P->d_tile_start_i, P->d_tile_end_i, T, chunk, 0,
-                                               P->d_tile_nitems);
-  b = P->cub_tmp_bytes;
-  CK(cub::DeviceScan::ExclusiveSum(P->d_cub_tmp, b, P->d_tile_nitems, P->d_tile_item_off, T, st));
-  k_emit_items<<<blocks_for(T), 256, 0, st>>>(P->d_slices, P->nslices, P->d_tile_start_i,
-                                              P->d_tile_end_i, P->d_tile_nitems, P->d_tile_item_off,
-                                              T, chunk, P->d_items_i, nullptr, P->d_counts, 0, -1,
-                                              0);
-  k_item_counts<<<blocks_for(TG), 256, 0, st>>>(P->d_tile_start_g, P->d_tile_end_g, TG, gchunk, 1,
-                                                P->d_tile_nitems);
-  b = P->cub_tmp_bytes;
-  CK(cub::DeviceScan::ExclusiveSum(P->d_cub_tmp, b, P->d_tile_nitems, P->d_tile_item_off, TG, st));
-  k_emit_items<<<blocks_for(TG), 256, 0, st>>>(P->d_slices, P->nslices, P->d_tile_start_g,
-                                               P->d_tile_end_g, P->d_tile_nitems, P->d_tile_item_off,
-                                               TG, gchunk, P->d_items_g, P->d_split_tiles, P->d_counts,
-                                               1, 3, 1);
-  CK(cudaGetLastError());
+  const int64_t max_items = std::max(max_items_i, max_items_g);
+  if (P->cap_sort < max_items) {
+    RK(dev_alloc(&P->d_items_tmp, (size_t)max_items));
+    for (int k = 0; k < 2; ++k) {
+      RK(dev_alloc(&P->d_sort_key[k], (size_t)max_items));
+      RK(dev_alloc(&P->d_sort_idx[k], (size_t)max_items));
+    }
+    P->cap_sort = max_items;
+  }
+  const int64_t part_elems = max_slots * (int64_t)P->max_coil * grid_tile_cells(P);
+  if (P->cap_part < part_elems) {
+    RK(dev_alloc(&P->d_part, (size_t)part_elems));
+    P->cap_part = part_elems;
+  }
+  {
+    size_t nb = 0;
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, nb, P->d_sort_key[0], P->d_sort_key[1],
+                                              P->d_sort_idx[0], P->d_sort_idx[1],
+                                              (int)std::max<int64_t>(max_items, 1), 0, 32, st);
+    RK(ensure_cub(P, std::max(nb, P->cub_tmp_bytes)));
+  }
+  // Emit into the staging list (padding pre-filled with slice = -1), then
+  // order longest first: CTAs start in index order, so the last wave holds
+  // short items instead of a few long tiles.
+  auto make_items = [&](int ntiles, int ch, int min_items, int64_t cap, int count_slot, int gridding,
+                        const int* tstart, const int* tend, Item* out) -> int {
+    if (cap == 0) return MRN_OK;
+    CK(cudaMemsetAsync(P->d_items_tmp, 0xff, (size_t)cap * sizeof(Item), st));
+    k_item_counts<<<blocks_for(ntiles), 256, 0, st>>>(tstart, tend, ntiles, ch, min_items,
+                                                      P->d_tile_nitems);
+    size_t nb = P->cub_tmp_bytes;
+    CK(cub::DeviceScan::ExclusiveSum(P->d_cub_tmp, nb, P->d_tile_nitems, P->d_tile_item_off, ntiles, st));
+    k_emit_items<<<blocks_for(ntiles), 256, 0, st>>>(P->d_slices, P->nslices, tstart, tend,
+                                                     P->d_tile_nitems, P->d_tile_item_off, ntiles, ch,
+                                                     P->d_items_tmp, P->d_split_tiles, P->d_counts,
+                                                     count_slot, gridding);
+    k_item_keys<<<blocks_for(cap), 256, 0, st>>>(P->d_items_tmp, cap, P->d_sort_key[0], P->d_sort_idx[0]);
+    CK(cudaGetLastError());
+    int kbits = 1;
+    while (kbits < 32 && (1ll << kbits) <= (long long)ch + 1) ++kbits;
+    nb = P->cub_tmp_bytes;
+    CK(cub::DeviceRadixSort::SortPairsDescending(P->d_cub_tmp, nb, P->d_sort_key[0], P->d_sort_key[1],
+                                                 P->d_sort_idx[0], P->d_sort_idx[1], (int)cap, 0, kbits,
+                                                 st));
+    k_gather_items<<<blocks_for(cap), 256, 0, st>>>(P->d_items_tmp, P->d_sort_idx[1], cap, out);
+    CK(cudaGetLastError());
+    return MRN_OK;
+  };
+  RK(make_items(T, chunk, 0, max_items_i, 0, 0, P->d_tile_start_i, P->d_tile_end_i, P->d_items_i));
+  RK(make_items(TG, gchunk, 1, max_items_g, 1, 1, P->d_tile_start_g, P->d_tile_end_g, P->d_items_g));
   RK(build_wtabs(P, st));
-  int hc[4] = {0, 0, 0, 0};
-  CK(cudaMemcpyAsync(hc, P->d_counts, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  P->n_items_interp = hc[0];
-  P->n_items_grid = hc[1];
-  P->n_split = hc[3];
-  // Longest items first: CTAs are dispatched in index order, so the last wave
-  // then consists of short items instead of a few long tiles.
-  RK(sort_items_longest_first(P->d_items_i, P->n_items_interp, st));
-  RK(sort_items_longest_first(P->d_items_g, P->n_items_grid, st));
+  P->n_items_interp = max_items_i;
+  P->n_items_grid = max_items_g;
+  P->n_split = max_split;
   P->traj_set = true;
   return MRN_OK;
 }

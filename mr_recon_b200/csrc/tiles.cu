@@ -16,9 +16,9 @@
 //     cooperatively by its G lanes, and reused for all coils;
 //   * gridding accumulates in shared memory (float atomics) and each tile is
 //     written back once with plain coalesced stores -- no global atomics and
-//     no zero fill of the output, except for tiles so dense that they were
-//     split over several CTAs (those are zeroed first and combined with
-//     global atomics).
+//     no zero fill of the output. Tiles so dense that they were split over
+//     several CTAs get one partial tile per CTA, summed in item order by a
+//     reduction pass, so every gridding path gives the same bits run to run.
 // Tap selection and weights follow the reference exactly: taps j = lo + q,
 // lo = ceil(u - W/2), valid iff |(float)j - u| <= W/2 (kernels.py:268-393),
 // weight = prod_d KB(|j_d - u_d| / (W_d/2)) (norm '1'), cells wrap circularly.
@@ -117,6 +117,7 @@ k_interp(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBPar
   float* wts = reinterpret_cast<float*>(tile + (size_t)cg * pstride);
 
   const Item it = items[blockIdx.x];
+  if (it.slice < 0) return;  // padding past the real items
   const SliceGeom& g = sl[it.slice];
   const int c0 = blockIdx.y * cg;
   const int ncoil = g.ncoil;
@@ -273,7 +274,7 @@ k_grid(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBParam
        const float4* __restrict__ coord, const int* __restrict__ perm,
        const float2* __restrict__ ksp, const float* __restrict__ dcf,
        const float2* __restrict__ temporal, float2* __restrict__ grid, int layout, float scale,
-       int cg, int pstride) {
+       int cg, int pstride, SplitOut so) {
   constexpr int SLOTS = 32 / G;
   constexpr int CPL = (G >= 32) ? 2 : 1;
   extern __shared__ float4 smem_f4[];
@@ -283,6 +284,7 @@ k_grid(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBParam
   int* locs = reinterpret_cast<int*>(wts + kWarps * D * KM * SLOTS);
 
   const Item it = items[blockIdx.x];
+  if (it.slice < 0) return;  // padding past the real items
   const SliceGeom& g = sl[it.slice];
   const int c0 = blockIdx.y * cg;
   if (c0 >= g.ncoil) return;
@@ -421,7 +423,7 @@ k_grid(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBParam
   }
   __syncthreads();
 
-  // write-back: one store per cell (or a global atomic for split tiles)
+  // write-back: one store per cell (into the item's partial slot for split tiles)
   int hs[kMaxDim];
   for (int i = 0; i < kMaxDim; ++i) hs[i] = (i < D && layout == kInternal) ? g.hshift[i] : 0;
   const int64_t goff = (layout == kInternal ? g.grid_off : g.ugrid_off) + (int64_t)c0 * g.gos;
@@ -440,25 +442,27 @@ k_grid(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBParam
     for (int q = lane; q < inner; q += 32) {
       const int s = pos_mod(f.org[D - 1] + q - hs[D - 1], g.nos[D - 1]);
       const float2 v = make_float2(sre[q], sim[q]);
-      if (it.split) {
-        atomicAdd(&dst[s].x, v.x);
-        atomicAdd(&dst[s].y, v.y);
-      } else {
-        dst[s] = v;
-      }
+      if (it.split) *split_slot(so, it.split, c0 + c, orow * inner + q) = v;
+      else dst[s] = v;
     }
   }
 }
 
-// Zero every coil plane of the split gridding tiles before their items run.
-constexpr int kZeroCoils = 8;
+// Sum the partial tiles of every split gridding tile in item order and store
+// the result: one CTA per (split tile, group of kSplitCoils coils), threads
+// over (coil, cell), each thread adding the tile's slots first to last. The
+// gridding kernels ran before on the same stream and wrote every slot read
+// here (a split tile's items are slots base .. base + n - 1).
+constexpr int kSplitCoils = 8;
 
 template <int D>
-__global__ void k_zero_split(const int* __restrict__ split_tiles, const int* __restrict__ counts,
-                             const SliceGeom* __restrict__ sl, int ns, float2* __restrict__ grid,
-                             int layout) {
+__global__ void __launch_bounds__(256)
+k_reduce_split(const int4* __restrict__ split_tiles, const int* __restrict__ counts,
+               const SliceGeom* __restrict__ sl, int ns, SplitOut so, float2* __restrict__ grid,
+               int layout) {
   if ((int)blockIdx.x >= counts[3]) return;
-  const int t = split_tiles[blockIdx.x];
+  const int4 sp = split_tiles[blockIdx.x];
+  const int t = sp.x, base = sp.y, nparts = sp.z;
   int s = 0;
   {
     int lo = 0, hi = ns - 1;
@@ -474,16 +478,22 @@ __global__ void k_zero_split(const int* __restrict__ split_tiles, const int* __r
   for (int i = 0; i < kMaxDim; ++i) hs[i] = (i < D && layout == kInternal) ? g.hshift[i] : 0;
   int cells = 1;
   for (int i = 0; i < D; ++i) cells *= f.size[i];
-  // one CTA per (split tile, group of kZeroCoils coils)
-  const int cbeg = blockIdx.y * kZeroCoils;
-  const int ncl = min(kZeroCoils, g.ncoil - cbeg);
+  const int cbeg = blockIdx.y * kSplitCoils;
+  const int ncl = min(kSplitCoils, g.ncoil - cbeg);
   if (ncl <= 0) return;
   const int64_t goff = (layout == kInternal ? g.grid_off : g.ugrid_off) + (int64_t)cbeg * g.gos;
   for (int idx = threadIdx.x; idx < ncl * cells; idx += blockDim.x) {
     const int c = idx / cells, cell = idx - c * cells;
+    const float2* src = split_slot(so, base + 1, cbeg + c, cell);
+    float2 acc = src[0];
+    for (int q = 1; q < nparts; ++q) {
+      const float2 v = src[(int64_t)q * so.slot_stride];
+      acc.x += v.x;
+      acc.y += v.y;
+    }
     int64_t lin;
     tile_storage<D>(g, f, hs, cell, &lin);
-    grid[goff + (int64_t)c * g.gos + lin] = make_float2(0.f, 0.f);
+    grid[goff + (int64_t)c * g.gos + lin] = acc;
   }
 }
 
@@ -505,6 +515,7 @@ k_traj_grad(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
   float* dws = wts + kWarps * D * KM * SLOTS;
 
   const Item it = items[blockIdx.x];
+  if (it.slice < 0) return;  // padding past the real items
   const SliceGeom& g = sl[it.slice];
   const int c0 = blockIdx.y * cg;
   if (c0 >= g.ncoil) return;
@@ -774,21 +785,27 @@ int launch_grid(mrn_plan* P, const float2* ksp, const float* dcf, GridLayout lay
   return launch_grid_t(P, ksp, dcf, nullptr, layout, grid, scale, st);
 }
 
-int launch_grid_t(mrn_plan* P, const float2* ksp, const float* dcf, const float2* temporal,
-                  GridLayout layout, float2* grid, float scale, cudaStream_t st) {
-  if (P->n_items_grid == 0) return MRN_OK;
+static int launch_reduce_split(mrn_plan* P, GridLayout layout, float2* grid, cudaStream_t st) {
+  if (P->n_split == 0) return MRN_OK;
+  const dim3 nb((unsigned)P->n_split, (unsigned)((P->max_coil + kSplitCoils - 1) / kSplitCoils));
+  const SplitOut so = split_out(P);
+  if (P->ndim == 1)
+    k_reduce_split<1><<<nb, 256, 0, st>>>(P->d_split_tiles, P->d_counts, P->d_slices, P->nslices, so, grid, (int)layout);
+  else if (P->ndim == 2)
+    k_reduce_split<2><<<nb, 256, 0, st>>>(P->d_split_tiles, P->d_counts, P->d_slices, P->nslices, so, grid, (int)layout);
+  else
+    k_reduce_split<3><<<nb, 256, 0, st>>>(P->d_split_tiles, P->d_counts, P->d_slices, P->nslices, so, grid, (int)layout);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? MRN_OK : cuda_fail(e);
+}
+
+// Items that own their tile store it; items of split tiles store partial
+// tiles, which the reduction pass afterwards sums into the grid.
+static int launch_grid_items(mrn_plan* P, const float2* ksp, const float* dcf, const float2* temporal,
+                             GridLayout layout, float2* grid, float scale, cudaStream_t st) {
   const bool fast = P->use_fast && fast_path_ok(P, true);
   const Layout L = plan_layout(P, 1, fast);
   const int G = pick_g(L.cg);
-  if (P->n_split > 0) {
-    const dim3 nb((unsigned)P->n_split, (unsigned)((P->max_coil + kZeroCoils - 1) / kZeroCoils));
-    if (P->ndim == 1)
-      k_zero_split<1><<<nb, 256, 0, st>>>(P->d_split_tiles, P->d_counts, P->d_slices, P->nslices, grid, (int)layout);
-    else if (P->ndim == 2)
-      k_zero_split<2><<<nb, 256, 0, st>>>(P->d_split_tiles, P->d_counts, P->d_slices, P->nslices, grid, (int)layout);
-    else
-      k_zero_split<3><<<nb, 256, 0, st>>>(P->d_split_tiles, P->d_counts, P->d_slices, P->nslices, grid, (int)layout);
-  }
   dim3 gridDim((unsigned)P->n_items_grid, (unsigned)((P->max_coil + L.cg - 1) / L.cg));
   if (fast && P->ndim == 3 && grid_reg3_ok(P))
     return launch_grid_reg3(P, ksp, dcf, temporal, (int)layout, grid, scale, st);
@@ -802,17 +819,26 @@ int launch_grid_t(mrn_plan* P, const float2* ksp, const float* dcf, const float2
     return launch_grid_fast(P, ksp, dcf, temporal, (int)layout, grid, scale, L.cg, G, L.pstride, L.smem,
                             gridDim, st);
   int rc = MRN_OK;
+  const SplitOut so = split_out(P);
   MRN_DISPATCH_DK(P->ndim, P->tap_max, MRN_DISPATCH_G(G, {
     auto kern = k_grid<DD, GG, KK>;
     rc = prepare(kern, L.smem);
     if (rc == MRN_OK)
       kern<<<gridDim, kThreads, L.smem, st>>>(P->d_items_g, P->d_slices, P->kb, P->d_coord_g,
                                               P->d_perm_g, ksp, dcf, temporal, grid, (int)layout,
-                                              scale, L.cg, L.pstride);
+                                              scale, L.cg, L.pstride, so);
   }));
   if (rc != MRN_OK) return rc;
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? MRN_OK : cuda_fail(e);
+}
+
+int launch_grid_t(mrn_plan* P, const float2* ksp, const float* dcf, const float2* temporal,
+                  GridLayout layout, float2* grid, float scale, cudaStream_t st) {
+  if (P->n_items_grid == 0) return MRN_OK;
+  const int rc = launch_grid_items(P, ksp, dcf, temporal, layout, grid, scale, st);
+  if (rc != MRN_OK) return rc;
+  return launch_reduce_split(P, layout, grid, st);
 }
 
 int launch_traj_grad(mrn_plan* P, const float2* grid, GridLayout layout, const float2* samples,

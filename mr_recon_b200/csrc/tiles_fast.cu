@@ -170,6 +170,7 @@ k_interp_fast(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, 
   float2* tile = reinterpret_cast<float2*>(smem_f4);
 
   const Item it = items[blockIdx.x];
+  if (it.slice < 0) return;  // padding past the real items
   const SliceGeom* gp = sl + it.slice;
   const int ncoil = gp->ncoil;
   const int c0 = blockIdx.y * cg;
@@ -283,7 +284,7 @@ k_grid_fast(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
             const float4* __restrict__ coord, const int* __restrict__ perm,
             const float2* __restrict__ ksp, const float* __restrict__ dcf,
             const float2* __restrict__ temporal, float2* __restrict__ grid, int layout, float scale,
-            int cg, int pstride) {
+            int cg, int pstride, SplitOut so) {
   constexpr int SLOTS = 32 / G;
   constexpr int CPL = G == 32 ? 2 : 1;
   constexpr int STRIDE = kWarps * SLOTS;
@@ -292,6 +293,7 @@ k_grid_fast(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
   float* acc_im = acc_re + (size_t)cg * pstride;
 
   const Item it = items[blockIdx.x];
+  if (it.slice < 0) return;  // padding past the real items
   const SliceGeom* gp = sl + it.slice;
   const int ncoil = gp->ncoil;
   const int c0 = blockIdx.y * cg;
@@ -432,12 +434,8 @@ k_grid_fast(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
       int s = s_first + q;
       if (s >= nl) s -= nl;
       const float2 v = make_float2(sre[q], sim[q]);
-      if (it.split) {
-        atomicAdd(&dst[s].x, v.x);
-        atomicAdd(&dst[s].y, v.y);
-      } else {
-        dst[s] = v;
-      }
+      if (it.split) *split_slot(so, it.split, c0 + c, orow * inner + q) = v;
+      else dst[s] = v;
     }
   }
 }
@@ -448,8 +446,8 @@ k_grid_fast(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
 // tap is a plain float32 shared-memory read-modify-write (LDS.64, 2 FFMA,
 // STS.64) -- no atomics (shared-memory float atomics are compare-and-swap
 // loops on sm_100a) and a fixed summation order, so results are bitwise
-// reproducible (except tiles split over several items, which combine with
-// global atomics).
+// reproducible (tiles split over several items write partial tiles that a
+// reduction pass adds in item order).
 // ---------------------------------------------------------------------------
 template <int K, int CPL>
 __global__ void __launch_bounds__(32)
@@ -457,11 +455,12 @@ k_grid_warp(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
             const float4* __restrict__ coord, const int* __restrict__ perm,
             const float2* __restrict__ ksp, const float* __restrict__ dcf,
             const float2* __restrict__ temporal, float2* __restrict__ grid, int layout, float scale,
-            int cg, int pstride) {
+            int cg, int pstride, SplitOut so) {
   extern __shared__ float4 smem_f4[];
   float2* acc = reinterpret_cast<float2*>(smem_f4);  // [cg][pstride]
 
   const Item it = items[blockIdx.x];
+  if (it.slice < 0) return;  // padding past the real items
   const SliceGeom* gp = sl + it.slice;
   const int ncoil = gp->ncoil;
   const int c0 = blockIdx.y * cg;
@@ -553,12 +552,8 @@ k_grid_warp(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
       const int s1 = wrap_once(f.org[1] + l1 - hs1, nos1);
       float2* d = dstc + (int64_t)s0 * nos1 + s1;
       const float2 v = src[cell];
-      if (it.split) {
-        atomicAdd(&d->x, v.x);
-        atomicAdd(&d->y, v.y);
-      } else {
-        *d = v;
-      }
+      if (it.split) *split_slot(so, it.split, c0 + c, cell) = v;
+      else *d = v;
     }
   }
 }
@@ -671,6 +666,7 @@ k_interp_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, K
   __shared__ int s_p[kInterpStage];     // their sample indices within the slice
 
   const Item it = items[blockIdx.x];
+  if (it.slice < 0) return;  // padding past the real items
   const SliceGeom* gp = sl + it.slice;
   const int ncoil = gp->ncoil;
   const int c0 = blockIdx.y * cg;
@@ -818,6 +814,7 @@ k_trajgrad_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl,
   __shared__ int s_p[kInterpStage];
 
   const Item it = items[blockIdx.x];
+  if (it.slice < 0) return;  // padding past the real items
   const SliceGeom* gp = sl + it.slice;
   const int ncoil = gp->ncoil;
   const int c0 = blockIdx.y * cg;
@@ -930,7 +927,8 @@ k_trajgrad_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl,
 // tile, so each lane keeps 4x8 complex cells in registers and every update
 // is a register FMA with a compile-time index: no shared-memory
 // read-modify-write, no atomics, float32 accumulation in a fixed order
-// (reproducible results).
+// (reproducible results; split tiles write partial tiles that a reduction
+// pass adds in item order).
 //
 // Entries run in batches of kRegBatch through an asynchronous pipeline
 // (cp.async), one barrier per batch. In iteration b:
@@ -975,7 +973,7 @@ k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBP
            const float4* __restrict__ coord, const int* __restrict__ perm,
            const float2* __restrict__ ksp, const float* __restrict__ dcf,
            const float2* __restrict__ temporal, float2* __restrict__ grid, int layout, float scale,
-           int cg) {
+           int cg, SplitOut so) {
   constexpr int T = kRegTile, R = kRegRows, B = kRegBatch, CW = 32 / SUB;
   __shared__ float4 s_c[3][B];      // coordinate ring
   __shared__ int s_pm[3][B];        // sample index ring
@@ -986,6 +984,7 @@ k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBP
   __shared__ float2 s_t[2][B];      // per entry: temporal weight
 
   const Item it = items[blockIdx.x];
+  if (it.slice < 0) return;  // padding past the real items
   const SliceGeom* gp = sl + it.slice;
   const int ncoil = gp->ncoil;
   const int c0 = blockIdx.y * cg;
@@ -1130,13 +1129,8 @@ k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBP
       if (b >= f.size[1]) break;
       int s = s1 + b;
       if (s >= nos1) s -= nos1;
-      float2* d = dst + rowo + s;
-      if (it.split) {
-        atomicAdd(&d->x, acc[a][b].x);
-        atomicAdd(&d->y, acc[a][b].y);
-      } else {
-        *d = acc[a][b];
-      }
+      if (it.split) *split_slot(so, it.split, c0 + coil, row * f.size[1] + b) = acc[a][b];
+      else dst[rowo + s] = acc[a][b];
     }
   }
 }
@@ -1152,8 +1146,9 @@ k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBP
 // memory, sample values copied asynchronously one batch ahead), in batches
 // of 64 entries; per batch each warp takes one ballot of the entries whose
 // footprint meets its x-plane and visits only those. Every y-row with a
-// weight takes 4 packed two-lane FMAs along z. No atomics except for split
-// tiles' write-back; float32 accumulation in a fixed order.
+// weight takes 4 packed two-lane FMAs along z. No atomics; float32
+// accumulation in a fixed order (split tiles write partial tiles that a
+// reduction pass adds in item order).
 // ---------------------------------------------------------------------------
 constexpr int kReg3Tile = 8;
 constexpr int kReg3Batch = 64;
@@ -1165,7 +1160,7 @@ k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
             const float4* __restrict__ coord, const int* __restrict__ perm,
             const float2* __restrict__ ksp, const float* __restrict__ dcf,
             const float2* __restrict__ temporal, float2* __restrict__ grid, int layout, float scale,
-            int cg) {
+            int cg, SplitOut so) {
   constexpr int T = kReg3Tile, B = kReg3Batch, CW = kReg3Coils;
   __shared__ float4 s_c[3][B];       // coordinate ring
   __shared__ int s_pm[3][B];         // sample index ring
@@ -1177,6 +1172,7 @@ k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
   __shared__ float2 s_t[2][B];       // per entry: temporal weight
 
   const Item it = items[blockIdx.x];
+  if (it.slice < 0) return;  // padding past the real items
   const SliceGeom* gp = sl + it.slice;
   const int ncoil = gp->ncoil;
   const int c0 = blockIdx.y * cg;
@@ -1327,13 +1323,10 @@ k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
       if (4 * half + b >= f.size[2]) break;
       int z = z0 + 4 * half + b;
       if (z >= nos2) z -= nos2;
-      float2* d = rowp + z;
-      if (it.split) {
-        atomicAdd(&d->x, acc[a][b].x);
-        atomicAdd(&d->y, acc[a][b].y);
-      } else {
-        *d = acc[a][b];
-      }
+      if (it.split)
+        *split_slot(so, it.split, c0 + coil, (warp * f.size[1] + y) * f.size[2] + 4 * half + b) = acc[a][b];
+      else
+        rowp[z] = acc[a][b];
     }
   }
 }
@@ -1420,7 +1413,8 @@ int launch_grid_warp(mrn_plan* P, const float2* ksp, const float* dcf, const flo
     rc = prep_attr(kern, smem);                                                                   \
     if (rc == MRN_OK)                                                                             \
       kern<<<gdim, 32, smem, st>>>(P->d_items_g, P->d_slices, P->kb, P->d_coord_g, P->d_perm_g,   \
-                                   ksp, dcf, temporal, grid, layout, scale, cg, pstride);         \
+                                   ksp, dcf, temporal, grid, layout, scale, cg, pstride,          \
+                                   split_out(P));                                                 \
   } while (0)
   const bool two = cg > 32;
   if (K == 5) { if (two) MRN_WARP_LAUNCH(5, 2); else MRN_WARP_LAUNCH(5, 1); }
@@ -1550,7 +1544,8 @@ int launch_grid_reg(mrn_plan* P, const float2* ksp, const float* dcf, const floa
   const int K = P->kb.ntaps[0];
 #define MRN_REG_LAUNCH(KK, SS)                                                              \
   k_grid_reg<KK, SS><<<gdim, 64, 0, st>>>(P->d_items_g, P->d_slices, P->kb, P->d_coord_g, \
-                                          P->d_perm_g, ksp, dcf, temporal, grid, layout, scale, cg)
+                                          P->d_perm_g, ksp, dcf, temporal, grid, layout, scale, cg, \
+                                          split_out(P))
 #define MRN_REG_SUB(KK)                     \
   if (sub == 4) MRN_REG_LAUNCH(KK, 4);      \
   else if (sub == 2) MRN_REG_LAUNCH(KK, 2); \
@@ -1581,7 +1576,7 @@ int launch_grid_reg3(mrn_plan* P, const float2* ksp, const float* dcf, const flo
   const int K = P->kb.ntaps[0];
 #define MRN_REG3_LAUNCH(KK)                                                                       \
   k_grid_reg3<KK><<<gdim, 256, 0, st>>>(P->d_items_g, P->d_slices, P->kb, P->d_coord_g, P->d_perm_g, \
-                                        ksp, dcf, temporal, grid, layout, scale, cg)
+                                        ksp, dcf, temporal, grid, layout, scale, cg, split_out(P))
   if (K == 5) MRN_REG3_LAUNCH(5);
   else if (K == 6) MRN_REG3_LAUNCH(6);
   else if (K == 7) MRN_REG3_LAUNCH(7);
@@ -1600,7 +1595,8 @@ int launch_grid_fast(mrn_plan* P, const float2* ksp, const float* dcf, const flo
     rc = prep_attr(kern, smem);
     if (rc == MRN_OK)
       kern<<<gdim, kThreads, smem, st>>>(P->d_items_g, P->d_slices, P->kb, P->d_coord_g, P->d_perm_g,
-                                         ksp, dcf, temporal, grid, layout, scale, cg, pstride);
+                                         ksp, dcf, temporal, grid, layout, scale, cg, pstride,
+                                         split_out(P));
   }));
   if (rc != MRN_OK) return rc;
   cudaError_t e = cudaGetLastError();

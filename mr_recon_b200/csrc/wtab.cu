@@ -137,6 +137,7 @@ k_interp_tab(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, i
   float2* tile = reinterpret_cast<float2*>(smem_f4);
 
   const Item it = items[blockIdx.x];
+  if (it.slice < 0) return;  // padding past the real items
   const SliceGeom* gp = sl + it.slice;
   const int ncoil = gp->ncoil;
   const int c0 = blockIdx.y * cg;
@@ -260,11 +261,13 @@ k_grid_warp_tab(const Item* __restrict__ items, const SliceGeom* __restrict__ sl
                 const int4* __restrict__ meta, const float4* __restrict__ tab,
                 const int* __restrict__ perm, const float2* __restrict__ ksp,
                 const float* __restrict__ dcf, const float2* __restrict__ temporal,
-                float2* __restrict__ grid, int layout, float scale, int cg, int pstride) {
+                float2* __restrict__ grid, int layout, float scale, int cg, int pstride,
+                SplitOut so) {
   extern __shared__ float4 smem_f4[];
   float2* acc = reinterpret_cast<float2*>(smem_f4);  // [cg][pstride]
 
   const Item it = items[blockIdx.x];
+  if (it.slice < 0) return;  // padding past the real items
   const SliceGeom* gp = sl + it.slice;
   const int ncoil = gp->ncoil;
   const int c0 = blockIdx.y * cg;
@@ -375,12 +378,8 @@ k_grid_warp_tab(const Item* __restrict__ items, const SliceGeom* __restrict__ sl
       const int s1 = wrap1(f.org[1] + l1 - hs1, nos1);
       float2* d = dstc + (int64_t)s0 * nos1 + s1;
       const float2 v = src[cell];
-      if (it.split) {
-        atomicAdd(&d->x, v.x);
-        atomicAdd(&d->y, v.y);
-      } else {
-        *d = v;
-      }
+      if (it.split) *split_slot(so, it.split, c0 + c, cell) = v;
+      else *d = v;
     }
   }
 }
@@ -389,7 +388,7 @@ k_grid_warp_tab(const Item* __restrict__ items, const SliceGeom* __restrict__ sl
 // Host side
 // ---------------------------------------------------------------------------
 bool wtab_applicable(const mrn_plan* P) {
-  if (!P->use_wtab || !P->use_fast || P->ndim != 2) return false;
+  if (!P->use_wtab || !P->use_fast || P->ndim != 2 || !P->kb.uniform_beta) return false;
   if (P->kb.ntaps[0] > 8 || P->kb.ntaps[1] > 8) return false;
   for (const auto& g : P->h_slices)
     for (int i = 0; i < 2; ++i)
@@ -473,7 +472,7 @@ int launch_grid_warp_tab(mrn_plan* P, const float2* ksp, const float* dcf, const
     rc = set_dynamic_smem(kern, smem);
     if (rc != MRN_OK) return;
     kern<<<gdim, 32, smem, st>>>(P->d_items_g, P->d_slices, P->d_wmeta_g, P->d_wtab_g, P->d_perm_g,
-                                 ksp, dcf, temporal, grid, layout, scale, cg, pstride);
+                                 ksp, dcf, temporal, grid, layout, scale, cg, pstride, split_out(P));
   };
   if (cg > 32) go(k_grid_warp_tab<2>);
   else go(k_grid_warp_tab<1>);

@@ -23,6 +23,25 @@ def _max_eigen(A, device, verbose):
     return me * 1.01
 
 
+def _fused_solver(A, max_iter, lamda_l2, max_eigen, tolerance, graph, ksp):
+    """The fused device CG of ``A`` for these solver settings. Solvers are kept
+    on the linop, keyed by the settings and the identity of its plan, coil maps
+    and density weights, so repeated calls (one per slice or frame) reuse the
+    buffers and, with ``graph=True``, the CUDA graph captured on the first call."""
+    key = (int(max_iter), float(lamda_l2), float(max_eigen), float(tolerance), bool(graph),
+           id(A.plan), id(A.mps), id(A.dcf))
+    cache = A.__dict__.setdefault("_fused_cg", {})
+    cg = cache.get(key)
+    if cg is None:
+        cg = SenseCG(A.plan, A.mps, A.dcf, max_iter, lamda_l2, max_eigen, tolerance)
+        if graph:
+            cg.ksp.copy_(ksp.reshape(-1))
+            cg.capture()
+        cache.clear()  # one solver per linop: a new setting replaces the old graph
+        cache[key] = cg
+    return cg
+
+
 def CG_SENSE_recon(A: linop, ksp: torch.Tensor, max_iter: Optional[int] = 15,
                    lamda_l2: Optional[float] = 0.0, max_eigen: Optional[float] = None,
                    tolerance: Optional[float] = 1e-8, weights: Optional[torch.Tensor] = None,
@@ -38,10 +57,7 @@ def CG_SENSE_recon(A: linop, ksp: torch.Tensor, max_iter: Optional[int] = 15,
         max_eigen = _max_eigen(A, device, verbose)
     fused = getattr(A, "plan", None) is not None and weights is None and ahb_init is None
     if fused:
-        cg = SenseCG(A.plan, A.mps, A.dcf, max_iter, lamda_l2, max_eigen, tolerance)
-        if graph:
-            cg.ksp.copy_(ksp.reshape(-1))
-            cg.capture()
+        cg = _fused_solver(A, max_iter, lamda_l2, max_eigen, tolerance, graph, ksp)
         x = cg.solve(ksp.to(complex_dtype))
         return x.reshape(A.im_size).clone()
     start = time.perf_counter()

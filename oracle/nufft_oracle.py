@@ -568,6 +568,32 @@ def conjugate_gradient(AHA, AHb, num_iters=10, lamda_l2=0.0, tolerance=1e-8):
     return x.astype(C64)
 
 
+def conjugate_gradient_f32(AHA, AHb, num_iters=10, lamda_l2=0.0, tolerance=1e-8):
+    """algs.py:779-872 in the reference's own arithmetic: complex64 iterates,
+    float32 sums for <p, Ap>, <r, z> and |r| (torch.sum on complex64), pAp
+    taken to a Python float (.item(), :845), alpha and beta float32."""
+    op = lambda v: (AHA(v) + np.complex64(lamda_l2) * v).astype(C64)
+    x = AHb.astype(C64).copy()
+    if num_iters == 0:
+        return x
+    r = (AHb.astype(C64) - op(x)).astype(C64)
+    z = r
+    p = z.copy()
+    for _ in range(num_iters):
+        Ap = op(p)
+        pAp = float(np.real(np.sum(np.conj(p) * Ap, dtype=C64)))
+        rz = np.float32(np.real(np.sum(np.conj(r) * z, dtype=C64)))
+        alpha = np.float32(rz / np.float32(pAp))
+        x = (x + alpha * p).astype(C64)
+        r = (r - alpha * Ap).astype(C64)
+        if np.linalg.norm(r) < tolerance:
+            break
+        z = r
+        beta = np.float32(np.float32(np.real(np.sum(np.conj(r) * z, dtype=C64))) / rz)
+        p = (z + beta * p).astype(C64)
+    return x
+
+
 def cg_sense(A: SenseOracle, ksp, max_iter, lamda_l2, max_eigen, tolerance=1e-8):
     """recons.py:77-156 with max_eigen given (no power method)."""
     AHb = A.adjoint(ksp.astype(C64)).astype(np.complex128) / max_eigen ** 0.5

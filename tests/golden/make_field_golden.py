@@ -3,7 +3,7 @@ reference's own ``b0_to_phis_alphas`` and ``alpha_segementation``
 (src/mr_recon/imperfections/field.py:58-96, 272-369) through the import shims
 in ``refshim.py``. Run once, by hand, where the reference source tree exists:
 
-    python tests/golden/make_field_golden.py /root/reference/src
+    python tests/golden/make_field_golden.py <reference>/src
 
 Writes ``field.npz`` next to this script; the tests never import the reference.
 """
@@ -46,4 +46,6 @@ def main(ref_src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python %s <reference>/src  (the mr_recon source tree)" % sys.argv[0])
+    main(sys.argv[1])

@@ -5,7 +5,7 @@ Runs the unmodified mr_recon package (its CPU torch fallback path:
 through the import shims in ``refshim.py``, and writes ``*.npz`` fixtures next
 to this script. Needs the reference source tree; it is run once, by hand:
 
-    python tests/golden/make_golden.py /root/reference/src
+    python tests/golden/make_golden.py <reference>/src
 
 The fixtures are small (a few hundred KB in total) and committed; the tests
 never import the reference.
@@ -179,4 +179,6 @@ def main(ref_src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python %s <reference>/src  (the mr_recon source tree)" % sys.argv[0])
+    main(sys.argv[1])

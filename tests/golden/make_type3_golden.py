@@ -5,7 +5,7 @@ through the import shims in ``refshim.py``. The reference's Kaiser-Bessel
 no fixture; its restatement is pinned to these exact sums instead. Run once,
 by hand, where the reference source tree exists:
 
-    python tests/golden/make_type3_golden.py /root/reference/src
+    python tests/golden/make_type3_golden.py <reference>/src
 
 Writes ``type3.npz`` next to this script; the tests never import the reference.
 """
@@ -50,4 +50,6 @@ def main(ref_src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python %s <reference>/src  (the mr_recon source tree)" % sys.argv[0])
+    main(sys.argv[1])

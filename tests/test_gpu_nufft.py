@@ -187,7 +187,7 @@ def test_oracle_parity_forward_adjoint_stages(case, path):
 
 def test_split_heavy_tiles_match_oracle():
     """A dense cluster of samples with a tiny work-item size forces tiles to be
-    split over many CTAs (zero pre-pass + atomic write-back in gridding)."""
+    split over many CTAs (partial tiles summed in item order in gridding)."""
     rng = np.random.RandomState(7)
     im = (48, 48)
     trj = np.concatenate([(rng.rand(1, 4000, 2) - 0.5) * 3.0, (rng.rand(1, 1000, 2) - 0.5) * 48], 1).astype(np.float32)
