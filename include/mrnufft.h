@@ -204,35 +204,31 @@ int mrn_sense_normal(mrn_plan* plan, const void* x, const void* mps, const float
 
 /*
  * Conjugate-gradient vector steps for n_slices independent systems (the loop
- * body of conjugate_gradient, algs.py:779-872). The iterates x, r, p are
- * complex128 (per-slice image layout, one image per slice); the operator
- * works on a complex64 copy p32 of p that these calls keep current, and its
- * result Ap is complex64. Dot products and norms are float64 sums in a fixed
- * order; per-slice scalars stay on the device, so a whole solve can be
- * captured in a CUDA graph and replays to the same bits as the eager solve.
- * (The reference runs CG in float32 vectors and dots; float64 iterates keep a
- * 20-iteration solve within ~1e-4 of float64 CG although the NUFFT is
- * complex64.) state: float64 [n_slices * 8] owned by the caller:
+ * body of conjugate_gradient, algs.py:779-872), complex64 vectors with
+ * float64 dot products and norms. Every float64 sum is taken in a fixed order
+ * (per-block partials added in block order), so a solve gives the same bits
+ * on every run, eager or replayed from a CUDA graph; per-slice scalars stay on
+ * the device, so a whole solve can be captured. Vectors use the per-slice
+ * image layout (one image per slice). state: float64 [n_slices * 8] owned by
+ * the caller:
  *   [0] rz  [1] pAp (accumulated)  [2] rr (accumulated)  [3] done  [4] tol^2
  *   [5] iterations  [6] last alpha  [7] last beta
- * mrn_cg_init : zero state; r = b - Ab (b, Ab complex64), p = r, x = b,
- *               p32 = p, rz = |r|^2
- * per iteration: Ap = (A^H A + lam) p32 accumulating Re<p32, Ap> into
- *                state[1] (mrn_sense_normal with pap = state + 1,
- *                pap_stride = 8), then
- * mrn_cg_step : alpha = rz/pAp; x += alpha p; r -= alpha Ap; rr = |r|^2;
- *               x32 = x (complex64) when x32 is not NULL
- * mrn_cg_dir  : done |= rr < tol^2; beta = rr/rz; p = r + beta p; p32 = p;
- *               rz = rr; pAp = rr = 0 for the next iteration
+ * mrn_cg_init : zero state; r = b - Ab (Ab given), p = r, x = b, rz = |r|^2
+ * per iteration: Ap = (A^H A + lam) p accumulating pAp into state[1]
+ *                (mrn_sense_normal with pap = state + 1, pap_stride = 8), then
+ * mrn_cg_step : alpha = rz/pAp; x += alpha p; r -= alpha Ap; rr = |r|^2
+ * mrn_cg_dir  : done |= rr < tol^2; beta = rr/rz; p = r + beta p; rz = rr;
+ *               pAp = rr = 0 for the next iteration
  * Once a slice is done its vectors are left unchanged (the reference breaks
  * out of the loop at the same point, algs.py:859-860).
  */
-int mrn_cg_init(mrn_plan* plan, const void* b, const void* Ab, void* x, void* r, void* p, void* p32,
+int mrn_cg_init(mrn_plan* plan, const void* b, const void* Ab, void* x, void* r, void* p,
                 double* state, double tol, void* stream);
-int mrn_cg_step(mrn_plan* plan, void* x, void* r, const void* p, const void* Ap, void* x32,
+int mrn_cg_step(mrn_plan* plan, void* x, void* r, const void* p, const void* Ap,
                 double* state, void* stream);
-int mrn_cg_dir(mrn_plan* plan, const void* r, void* p, void* p32, double* state, void* stream);
-/* Per-slice Re<a, b> in float64, accumulated into out[slice] (caller zeroes). */
+int mrn_cg_dir(mrn_plan* plan, const void* r, void* p, double* state, void* stream);
+/* Per-slice Re<a, b> in float64 (fixed summation order), accumulated into
+ * out[slice] (caller zeroes). */
 int mrn_cg_dot(mrn_plan* plan, const void* a, const void* b, double* out, void* stream);
 
 /*

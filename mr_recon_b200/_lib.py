@@ -71,9 +71,9 @@ SIGNATURES = {
     "mrn_sense_forward": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "mrn_sense_adjoint": (_i, [_vp, _vp, _vp, _vp, _vp, _f, _vp]),
     "mrn_sense_normal": (_i, [_vp, _vp, _vp, _vp, _vp, _f, _f, _vp, _i, _vp]),
-    "mrn_cg_init": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _d, _vp]),
-    "mrn_cg_step": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
-    "mrn_cg_dir": (_i, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "mrn_cg_init": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _d, _vp]),
+    "mrn_cg_step": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "mrn_cg_dir": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "mrn_cg_dot": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "mrn_interp_noalloc": (_i, [_i, _pi, _i, _i64, _pd, _d, _vp, _vp, _vp, _vp]),
 }

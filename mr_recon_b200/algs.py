@@ -42,48 +42,45 @@ def conjugate_gradient(AHA: Callable, AHb: torch.Tensor, P: Optional[Callable] =
                        tolerance: Optional[float] = 1e-8, return_resids: Optional[bool] = False,
                        weights: Optional[torch.Tensor] = None, verbose=True) -> torch.Tensor:
     """Complex CG for (AHA + lamda_l2 I) x = AHb starting at x0 = AHb
-    (algs.py:779-872). The iterates are kept in double width (complex128 for
-    a complex64 AHb) while AHA and P see and return AHb's dtype: a 20-iteration
-    solve then stays within ~1e-4 of float64 CG, where float32 iterates (the
-    reference) drift 1e-3..1e-2 from it. Returns AHb's dtype."""
-    dt = AHb.dtype
-    wide = torch.complex128 if dt == torch.complex64 else (torch.float64 if dt == torch.float32 else dt)
+    (algs.py:779-872): vectors in AHb's dtype, dot products and norms in
+    float64, and no host synchronisation per iteration (the stop test is a
+    device-side mask, where the reference calls .item() and breaks)."""
     if P is None:
         P = lambda x: x  # noqa: E731
-    Pw = lambda v: P(v.to(dt)).to(wide)  # noqa: E731
     if weights is not None:
-        op = lambda x: AHA(x.to(dt)).to(wide) + lamda_l2 * weights * x  # noqa: E731
+        op = lambda x: AHA(x) + lamda_l2 * weights * x  # noqa: E731
     else:
-        op = lambda x: AHA(x.to(dt)).to(wide) + lamda_l2 * x  # noqa: E731
-    x0 = AHb.to(wide)
+        op = lambda x: AHA(x) + lamda_l2 * x  # noqa: E731
+    x0 = AHb.clone()
     if num_iters == 0:
-        return x0.to(dt)
-    r = AHb.to(wide) - op(x0)
-    z = Pw(r)
+        return x0
+    r = AHb - op(x0)
+    z = P(r)
     p = z.clone()
     done = torch.zeros((), dtype=torch.bool, device=AHb.device)
+    real = x0.real.dtype if x0.is_complex() else x0.dtype
     if return_resids:
         resids = []
-        xs = [x0.to(dt)]
+        xs = [x0.clone()]
     for _ in tqdm(range(num_iters), "CG Iterations", disable=not verbose):
         Ap = op(p)
         pAp = _rdot(p, Ap)
         rz = _rdot(r, z)
-        alpha = torch.where(done, torch.zeros_like(rz), rz / pAp)
+        alpha = torch.where(done, torch.zeros_like(rz), rz / pAp).to(real)
         x0 = x0 + alpha * p
         r = r - alpha * Ap
         rr = _rdot(r, r)
         rnrm = rr.sqrt()
         if return_resids:
             resids.append(rnrm.item())
-            xs.append(x0.to(dt))
+            xs.append(x0.clone())
         done = done | (rnrm < tolerance)
-        z = Pw(r)
-        beta = torch.where(done, torch.zeros_like(rz), _rdot(r, z) / rz)
+        z = P(r)
+        beta = torch.where(done, torch.zeros_like(rz), _rdot(r, z) / rz).to(real)
         p = torch.where(done, p, z + beta * p)
     if return_resids:
         return resids, xs
-    return x0.to(dt)
+    return x0
 
 
 def power_method_operator(A: Callable, x0: torch.Tensor, num_iter: Optional[int] = 15,
@@ -156,9 +153,9 @@ def gradient_descent(AHA: Callable, AHb: torch.Tensor, lr: float, num_iters: Opt
 
 class SenseCG:
     """CG-SENSE (recons.py:77-156 with max_eigen given) on a fused plan: one
-    image per slice, every slice of the plan solved at once. The iterates are
-    complex128 and the NUFFT operator complex64 (mrn_cg_init documents why).
-    All scalars stay on the device (float64 state per slice), so ``capture()``
+    image per slice, every slice of the plan solved at once: complex64
+    vectors, float64 dot products and norms summed in a fixed order. All
+    scalars stay on the device (float64 state per slice), so ``capture()``
     can record the whole solve -- AHb, initial residual and ``max_iter``
     iterations -- in one CUDA graph, replayed by ``solve`` with the same bits
     as the eager solve.
@@ -183,9 +180,8 @@ class SenseCG:
         self.max_eigen = float(me[0])
         self.tol = float(tolerance)
         nx = sum(int(torch.tensor(s).prod()) for s in plan.im_sizes)
-        mk = lambda dt=complex_dtype: torch.zeros(nx, dtype=dt, device=dev)  # noqa: E731
-        self.b, self.Ap, self.p32, self.x32 = mk(), mk(), mk(), mk()
-        self.x, self.r, self.p = mk(torch.complex128), mk(torch.complex128), mk(torch.complex128)
+        mk = lambda: torch.zeros(nx, dtype=complex_dtype, device=dev)  # noqa: E731
+        self.b, self.x, self.r, self.p, self.Ap = mk(), mk(), mk(), mk(), mk()
         self.state = torch.zeros(n * 8, dtype=torch.float64, device=dev)
         self.ksp = torch.zeros(plan.n_ksp, dtype=complex_dtype, device=dev)
         self.graph = None
@@ -194,19 +190,17 @@ class SenseCG:
         pl = self.plan
         s_adj = 1.0 / self.max_eigen ** 0.5
         s_nrm = 1.0 / self.max_eigen
-        if self.max_iter == 0:
-            pl.sense_adjoint(self.ksp, self.dcf, self.mps, self.x32, s_adj)
-            return
         pl.sense_adjoint(self.ksp, self.dcf, self.mps, self.b, s_adj)
+        if self.max_iter == 0:
+            self.x.copy_(self.b)
+            return
         pl.sense_normal(self.b, self.mps, self.dcf, self.Ap, s_nrm, self.lam)
-        pl.cg_init(self.b, self.Ap, self.x, self.r, self.p, self.p32, self.state, self.tol)
-        # x32 is written by every step of a slice that is not done, and a
-        # slice's x no longer changes once it is, so x32 = x after step one
+        pl.cg_init(self.b, self.Ap, self.x, self.r, self.p, self.state, self.tol)
         pap = self.state[1:]
         for _ in range(self.max_iter):
-            pl.sense_normal(self.p32, self.mps, self.dcf, self.Ap, s_nrm, self.lam, pap, 8)
-            pl.cg_step(self.x, self.r, self.p, self.Ap, self.state, self.x32)
-            pl.cg_dir(self.r, self.p, self.p32, self.state)
+            pl.sense_normal(self.p, self.mps, self.dcf, self.Ap, s_nrm, self.lam, pap, 8)
+            pl.cg_step(self.x, self.r, self.p, self.Ap, self.state)
+            pl.cg_dir(self.r, self.p, self.state)
 
     def capture(self):
         """Record one full solve in a CUDA graph (after a warm-up run)."""
@@ -222,16 +216,15 @@ class SenseCG:
         return self
 
     def solve(self, ksp: Optional[torch.Tensor] = None) -> torch.Tensor:
-        """Run one solve on ``ksp`` (plan k-space layout); returns x as
-        complex64 (a view of an internal buffer, overwritten by the next
-        solve; the complex128 iterate is ``self.x``)."""
+        """Run one solve on ``ksp`` (plan k-space layout); returns x (a view
+        of an internal buffer, overwritten by the next solve)."""
         if ksp is not None:
             self.ksp.copy_(ksp.reshape(-1))
         if self.graph is not None:
             self.graph.replay()
         else:
             self._run()
-        return self.x32
+        return self.x
 
     def iterations(self) -> torch.Tensor:
         return self.state.view(-1, 8)[:, 5]

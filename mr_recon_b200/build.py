@@ -23,7 +23,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(PKG, "libmrnufft.so")
-HEADERS = [os.path.join(CSRC, f) for f in ("common.cuh", "internal.cuh")] + [
+HEADERS = [os.path.join(CSRC, f) for f in ("common.cuh", "internal.cuh", "tile_util.cuh")] + [
     os.path.join(ROOT, "include", "mrnufft.h")]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -7,11 +7,11 @@
 using namespace mrn;
 
 namespace mrn {
-int launch_cg_init(mrn_plan* P, const float2* b, const float2* Ab, double2* x, double2* r, double2* p,
-                   float2* p32, double* state, double tol, cudaStream_t st);
-int launch_cg_step(mrn_plan* P, double2* x, double2* r, const double2* p, const float2* Ap, float2* x32,
+int launch_cg_init(mrn_plan* P, const float2* b, const float2* Ab, float2* x, float2* r, float2* p,
+                   double* state, double tol, cudaStream_t st);
+int launch_cg_step(mrn_plan* P, float2* x, float2* r, const float2* p, const float2* Ap,
                    double* state, cudaStream_t st);
-int launch_cg_dir(mrn_plan* P, const double2* r, double2* p, float2* p32, double* state, cudaStream_t st);
+int launch_cg_dir(mrn_plan* P, const float2* r, float2* p, double* state, cudaStream_t st);
 int launch_cg_dot(mrn_plan* P, const float2* a, const float2* b, double* out, cudaStream_t st);
 }  // namespace mrn
 
@@ -130,26 +130,25 @@ int mrn_sense_normal(mrn_plan* P, const void* x, const void* mps, const float* d
                      lam, pap, pap_stride, ST(s));
 }
 
-int mrn_cg_init(mrn_plan* P, const void* b, const void* Ab, void* x, void* r, void* p, void* p32,
+int mrn_cg_init(mrn_plan* P, const void* b, const void* Ab, void* x, void* r, void* p,
                 double* state, double tol, void* s) {
-  if (!P || !b || !Ab || !x || !r || !p || !p32 || !state) return MRN_ERR_ARG;
+  if (!P || !b || !Ab || !x || !r || !p || !state) return MRN_ERR_ARG;
   StageTimer t(P, kStageCg, ST(s));
-  return launch_cg_init(P, (const float2*)b, (const float2*)Ab, (double2*)x, (double2*)r, (double2*)p,
-                        (float2*)p32, state, tol, ST(s));
+  return launch_cg_init(P, (const float2*)b, (const float2*)Ab, (float2*)x, (float2*)r, (float2*)p,
+                        state, tol, ST(s));
 }
 
-int mrn_cg_step(mrn_plan* P, void* x, void* r, const void* p, const void* Ap, void* x32,
-                double* state, void* s) {
+int mrn_cg_step(mrn_plan* P, void* x, void* r, const void* p, const void* Ap, double* state,
+                void* s) {
   if (!P || !x || !r || !p || !Ap || !state) return MRN_ERR_ARG;
   StageTimer t(P, kStageCg, ST(s));
-  return launch_cg_step(P, (double2*)x, (double2*)r, (const double2*)p, (const float2*)Ap, (float2*)x32,
-                        state, ST(s));
+  return launch_cg_step(P, (float2*)x, (float2*)r, (const float2*)p, (const float2*)Ap, state, ST(s));
 }
 
-int mrn_cg_dir(mrn_plan* P, const void* r, void* p, void* p32, double* state, void* s) {
-  if (!P || !r || !p || !p32 || !state) return MRN_ERR_ARG;
+int mrn_cg_dir(mrn_plan* P, const void* r, void* p, double* state, void* s) {
+  if (!P || !r || !p || !state) return MRN_ERR_ARG;
   StageTimer t(P, kStageCg, ST(s));
-  return launch_cg_dir(P, (const double2*)r, (double2*)p, (float2*)p32, state, ST(s));
+  return launch_cg_dir(P, (const float2*)r, (float2*)p, state, ST(s));
 }
 
 int mrn_cg_dot(mrn_plan* P, const void* a, const void* b, double* out, void* s) {

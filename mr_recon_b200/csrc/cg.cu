@@ -1,14 +1,10 @@
 // Conjugate-gradient vector steps for a batch of independent systems, one
 // image per slice (the loop body of conjugate_gradient, algs.py:779-872).
-// The iterates x, r, p are complex128: with float64 vectors the 20-iteration
-// CG-SENSE solve follows float64 CG to ~3e-5 although the normal operator
-// (the NUFFT) runs in complex64, while float32 vectors drift 1e-3 (float64
-// dots) to 2e-2 (float32 dots, the reference's arithmetic) from it. The
-// operator reads a complex64 copy of p that these kernels keep current. Every
-// dot product and norm is a float64 sum in a fixed order, and the per-slice
-// scalars never leave the device, so a solve can be captured in a CUDA graph
-// (the reference calls .item() every iteration, algs.py:845) and replays to
-// the same bits as the eager solve. State per slice, float64[8]:
+// Vectors are complex64; every dot product and norm is a float64 sum in a
+// fixed order (block partials added in block order by the last block), and
+// the per-slice scalars never leave the device, so a solve can be captured in
+// a CUDA graph (the reference calls .item() every iteration, algs.py:845) and
+// replays to the same bits as the eager solve. State per slice, float64[8]:
 //   [0] rz   [1] pAp (accumulated)   [2] rr (accumulated)   [3] done
 //   [4] tol^2   [5] iterations done   [6] alpha   [7] beta
 #include <algorithm>
@@ -54,13 +50,11 @@ __device__ __forceinline__ void slice_sums(double acc, double* __restrict__ part
   if (threadIdx.x == 0) *counter = 0u;
 }
 
-// r = b - Ab; p = r; x = b (complex128); p32 = p (complex64); state[0] += |r|^2;
-// state[4] = tol^2
+// r = b - Ab; p = r; x = b; state[0] += |r|^2; state[4] = tol^2
 __global__ void __launch_bounds__(kCgThreads)
 k_cg_init(const SliceGeom* __restrict__ sl, const float2* __restrict__ b, const float2* __restrict__ Ab,
-          double2* __restrict__ x, double2* __restrict__ r, double2* __restrict__ p,
-          float2* __restrict__ p32, double* __restrict__ state, double tol2, double* __restrict__ part,
-          unsigned* __restrict__ counter) {
+          float2* __restrict__ x, float2* __restrict__ r, float2* __restrict__ p,
+          double* __restrict__ state, double tol2, double* __restrict__ part, unsigned* __restrict__ counter) {
   __shared__ double red[kCgThreads / 32];
   const int s = blockIdx.y;
   const SliceGeom& g = sl[s];
@@ -69,72 +63,66 @@ k_cg_init(const SliceGeom* __restrict__ sl, const float2* __restrict__ b, const 
        i += (int64_t)gridDim.x * kCgThreads) {
     const int64_t k = g.x_off + i;
     const float2 bb = b[k], ab = Ab[k];
-    const double2 rr = make_double2((double)bb.x - ab.x, (double)bb.y - ab.y);
+    const float2 rr = make_float2(bb.x - ab.x, bb.y - ab.y);
     r[k] = rr;
     p[k] = rr;
-    p32[k] = make_float2((float)rr.x, (float)rr.y);
-    x[k] = make_double2(bb.x, bb.y);
-    acc += rr.x * rr.x + rr.y * rr.y;
+    x[k] = bb;
+    acc += (double)rr.x * rr.x + (double)rr.y * rr.y;
   }
   acc = block_sum(acc, red);
   if (threadIdx.x == 0 && blockIdx.x == 0) state[s * 8 + 4] = tol2;
   slice_sums(acc, part, counter, state + 0, 8, nullptr);
 }
 
-// alpha = rz / pAp; x += alpha p; r -= alpha Ap; state[2] += |r|^2 (skipped
-// when done); x32 = x (complex64) when given
+// alpha = rz / pAp; x += alpha p; r -= alpha Ap; state[2] += |r|^2 (skipped when done)
 __global__ void __launch_bounds__(kCgThreads)
-k_cg_step(const SliceGeom* __restrict__ sl, double2* __restrict__ x, double2* __restrict__ r,
-          const double2* __restrict__ p, const float2* __restrict__ Ap, float2* __restrict__ x32,
-          double* __restrict__ state, double* __restrict__ part, unsigned* __restrict__ counter) {
+k_cg_step(const SliceGeom* __restrict__ sl, float2* __restrict__ x, float2* __restrict__ r,
+          const float2* __restrict__ p, const float2* __restrict__ Ap, double* __restrict__ state,
+          double* __restrict__ part, unsigned* __restrict__ counter) {
   __shared__ double red[kCgThreads / 32];
   const int s = blockIdx.y;
   const SliceGeom& g = sl[s];
   const double* S = state + s * 8;
   double acc = 0.0;
   if (S[3] == 0.0) {
-    const double alpha = S[0] / S[1];
+    const float alpha = (float)(S[0] / S[1]);
     for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < g.nimg;
          i += (int64_t)gridDim.x * kCgThreads) {
       const int64_t k = g.x_off + i;
-      const double2 pp = p[k];
-      const float2 ap = Ap[k];
-      double2 xx = x[k], rr = r[k];
-      xx.x = fma(alpha, pp.x, xx.x);
-      xx.y = fma(alpha, pp.y, xx.y);
-      rr.x = fma(-alpha, (double)ap.x, rr.x);
-      rr.y = fma(-alpha, (double)ap.y, rr.y);
+      const float2 pp = p[k], ap = Ap[k];
+      float2 xx = x[k], rr = r[k];
+      xx.x = fmaf(alpha, pp.x, xx.x);
+      xx.y = fmaf(alpha, pp.y, xx.y);
+      rr.x = fmaf(-alpha, ap.x, rr.x);
+      rr.y = fmaf(-alpha, ap.y, rr.y);
       x[k] = xx;
       r[k] = rr;
-      if (x32) x32[k] = make_float2((float)xx.x, (float)xx.y);
-      acc += rr.x * rr.x + rr.y * rr.y;
+      acc += (double)rr.x * rr.x + (double)rr.y * rr.y;
     }
   }
   acc = block_sum(acc, red);
   slice_sums(acc, part, counter, state + 2, 8, state);
 }
 
-// done |= rr < tol^2; beta = rr / rz; p = r + beta p; p32 = p (complex64);
-// then (last block) rz = rr, pAp = rr = 0, iterations += 1.
+// done |= rr < tol^2; beta = rr / rz; p = r + beta p; then (last block) rz = rr,
+// pAp = rr = 0, iterations += 1.
 __global__ void __launch_bounds__(kCgThreads)
-k_cg_dir(const SliceGeom* __restrict__ sl, int ns, const double2* __restrict__ r,
-         double2* __restrict__ p, float2* __restrict__ p32, double* __restrict__ state,
-         unsigned* __restrict__ counter) {
+k_cg_dir(const SliceGeom* __restrict__ sl, int ns, const float2* __restrict__ r,
+         float2* __restrict__ p, double* __restrict__ state, unsigned* __restrict__ counter) {
   const int s = blockIdx.y;
   const SliceGeom& g = sl[s];
   double* S = state + s * 8;
   const bool done = S[3] != 0.0 || S[2] < S[4];
   if (!done) {
-    const double beta = S[2] / S[0];
+    const float beta = (float)(S[2] / S[0]);
     for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < g.nimg;
          i += (int64_t)gridDim.x * kCgThreads) {
       const int64_t k = g.x_off + i;
-      const double2 rr = r[k];
-      double2 pp = p[k];
-      pp.x = fma(beta, pp.x, rr.x);
-      pp.y = fma(beta, pp.y, rr.y);
+      const float2 rr = r[k];
+      float2 pp = p[k];
+      pp.x = fmaf(beta, pp.x, rr.x);
+      pp.y = fmaf(beta, pp.y, rr.y);
       p[k] = pp;
-      p32[k] = make_float2((float)pp.x, (float)pp.y);
     }
   }
   __syncthreads();
@@ -183,25 +171,25 @@ static dim3 cg_grid(const mrn_plan* P) {
   return dim3((unsigned)bx, (unsigned)P->nslices);
 }
 
-int launch_cg_init(mrn_plan* P, const float2* b, const float2* Ab, double2* x, double2* r, double2* p,
-                   float2* p32, double* state, double tol, cudaStream_t st) {
+int launch_cg_init(mrn_plan* P, const float2* b, const float2* Ab, float2* x, float2* r, float2* p,
+                   double* state, double tol, cudaStream_t st) {
   cudaError_t e = cudaMemsetAsync(state, 0, (size_t)P->nslices * 8 * sizeof(double), st);
   if (e != cudaSuccess) return cuda_fail(e);
-  k_cg_init<<<cg_grid(P), kCgThreads, 0, st>>>(P->d_slices, b, Ab, x, r, p, p32, state, tol * tol,
+  k_cg_init<<<cg_grid(P), kCgThreads, 0, st>>>(P->d_slices, b, Ab, x, r, p, state, tol * tol,
                                                 P->d_red, P->d_sync + 1);
   e = cudaGetLastError();
   return e == cudaSuccess ? MRN_OK : cuda_fail(e);
 }
 
-int launch_cg_step(mrn_plan* P, double2* x, double2* r, const double2* p, const float2* Ap, float2* x32,
-                   double* state, cudaStream_t st) {
-  k_cg_step<<<cg_grid(P), kCgThreads, 0, st>>>(P->d_slices, x, r, p, Ap, x32, state, P->d_red, P->d_sync + 1);
+int launch_cg_step(mrn_plan* P, float2* x, float2* r, const float2* p, const float2* Ap, double* state,
+                   cudaStream_t st) {
+  k_cg_step<<<cg_grid(P), kCgThreads, 0, st>>>(P->d_slices, x, r, p, Ap, state, P->d_red, P->d_sync + 1);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? MRN_OK : cuda_fail(e);
 }
 
-int launch_cg_dir(mrn_plan* P, const double2* r, double2* p, float2* p32, double* state, cudaStream_t st) {
-  k_cg_dir<<<cg_grid(P), kCgThreads, 0, st>>>(P->d_slices, P->nslices, r, p, p32, state, P->d_sync);
+int launch_cg_dir(mrn_plan* P, const float2* r, float2* p, double* state, cudaStream_t st) {
+  k_cg_dir<<<cg_grid(P), kCgThreads, 0, st>>>(P->d_slices, P->nslices, r, p, state, P->d_sync);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? MRN_OK : cuda_fail(e);
 }

@@ -20,46 +20,11 @@
 
 #include "common.cuh"
 #include "internal.cuh"
+#include "tile_util.cuh"
 
 namespace mrn {
 
 namespace {
-
-struct Frame {
-  int org[kMaxDim];
-  int size[kMaxDim];
-};
-
-__device__ __forceinline__ Frame frame_of(const SliceGeom& g, int tile, int D, bool gridding) {
-  Frame f;
-  int rem = tile;
-  int tc[kMaxDim] = {0, 0, 0};
-  const int* nts = gridding ? g.gntile : g.ntile;
-  for (int i = D - 1; i >= 0; --i) {
-    tc[i] = rem % nts[i];
-    rem /= nts[i];
-  }
-#pragma unroll
-  for (int i = 0; i < kMaxDim; ++i) {
-    if (i < D) {
-      f.org[i] = tile_begin(tc[i], g.nos[i], nts[i]);
-      f.size[i] = tile_begin(tc[i] + 1, g.nos[i], nts[i]) - f.org[i];
-    } else {
-      f.org[i] = 0;
-      f.size[i] = 1;
-    }
-  }
-  return f;
-}
-
-__device__ __forceinline__ int wrap_once(int a, int n) {
-  // a in (-n, 2n): a mod n
-  a = a < 0 ? a + n : a;
-  return a >= n ? a - n : a;
-}
-
-template <class T>
-__device__ __forceinline__ T sel3(const T* v, int i) { return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]); }
 
 // a mod n for a in (-n, inf), by subtraction (region rows may wrap more than once on tiny grids)
 __device__ __forceinline__ int wrap_cells(int a, int n) {
@@ -951,22 +916,6 @@ constexpr int kRegTile = 8;
 constexpr int kRegRows = kRegTile / 2;  // tile rows per warp
 constexpr int kRegBatch = 16;
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
 template <int K, int SUB>
 __global__ void __launch_bounds__(64, 8)
 k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBParams kb,
@@ -1131,202 +1080,6 @@ k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBP
       if (s >= nos1) s -= nos1;
       if (it.split) *split_slot(so, it.split, c0 + coil, row * f.size[1] + b) = acc[a][b];
       else dst[rowo + s] = acc[a][b];
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// 3D gridding with the tile accumulator in registers. One CTA of 8 warps per
-// work item and group of at most 16 coils; the tile is at most 8x8x8 cells.
-// Warp w owns x-plane w, half-warp h owns z-cells 4h..4h+3, lane = coil, so
-// each thread keeps 8 (y) x 4 (z) complex cells in registers and the y-rows
-// are the same for the whole warp (a row without weight is skipped by a
-// warp-uniform branch). Same pipeline as the 2D kernel (coordinates through
-// a cp.async ring, tile-aligned 1D weights computed once per entry in shared
-// memory, sample values copied asynchronously one batch ahead), in batches
-// of 64 entries; per batch each warp takes one ballot of the entries whose
-// footprint meets its x-plane and visits only those. Every y-row with a
-// weight takes 4 packed two-lane FMAs along z. No atomics; float32
-// accumulation in a fixed order (split tiles write partial tiles that a
-// reduction pass adds in item order).
-// ---------------------------------------------------------------------------
-constexpr int kReg3Tile = 8;
-constexpr int kReg3Batch = 64;
-constexpr int kReg3Coils = 16;
-
-template <int K>
-__global__ void __launch_bounds__(256, 2)
-k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBParams kb,
-            const float4* __restrict__ coord, const int* __restrict__ perm,
-            const float2* __restrict__ ksp, const float* __restrict__ dcf,
-            const float2* __restrict__ temporal, float2* __restrict__ grid, int layout, float scale,
-            int cg, SplitOut so) {
-  constexpr int T = kReg3Tile, B = kReg3Batch, CW = kReg3Coils;
-  __shared__ float4 s_c[3][B];       // coordinate ring
-  __shared__ int s_pm[3][B];         // sample index ring
-  __shared__ float4 s_wx[2][B][2];   // per entry: x weights x scale (cells 0-7)
-  __shared__ float4 s_wy[2][B][2];   // per entry: y weights (cells 0-3, 4-7)
-  __shared__ float4 s_wz[2][B][4];   // per entry: z weights, each twice
-  __shared__ float2 s_v[2][B][CW];   // per entry and coil: sample value
-  __shared__ float s_d[2][B];        // per entry: density weight
-  __shared__ float2 s_t[2][B];       // per entry: temporal weight
-
-  const Item it = items[blockIdx.x];
-  if (it.slice < 0) return;  // padding past the real items
-  const SliceGeom* gp = sl + it.slice;
-  const int ncoil = gp->ncoil;
-  const int c0 = blockIdx.y * cg;
-  if (c0 >= ncoil) return;
-  const int ncg = min(cg, ncoil - c0);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int half = lane >> 4, coil = lane & 15;
-  const bool has_coil = coil < ncg;
-  const Frame f = frame_of(*gp, it.tile, 3, true);
-  const int64_t m = gp->m, pt_off = gp->pt_off;
-  const float2* kspg = ksp + gp->ksp_off + (int64_t)c0 * m;
-  const int nbatch = (it.count + B - 1) / B;
-  auto batch_len = [&](int bi) { return bi < nbatch ? min(B, it.count - bi * B) : 0; };
-
-  auto copy_coords = [&](int bi) {
-    const int nb = batch_len(bi), r3 = bi % 3;
-    if (tid < nb) cp_async16(&s_c[r3][tid], coord + it.start + bi * B + tid);
-    else if (tid >= B && tid - B < nb) cp_async4(&s_pm[r3][tid - B], perm + it.start + bi * B + tid - B);
-  };
-  // thread = (entry j and j + 16, coil c): one 8-byte copy per entry and coil
-  auto copy_values = [&](int bi) {
-    const int nb = batch_len(bi), b2 = bi & 1, r3 = bi % 3;
-    const int c = tid & 15;
-#pragma unroll
-    for (int j = tid >> 4; j < B; j += 16)
-      if (j < nb && c < ncg) cp_async8(&s_v[b2][j][c], kspg + (int64_t)c * m + (s_pm[r3][j] - pt_off));
-    if (tid < nb) {
-      if (dcf) cp_async4(&s_d[b2][tid], dcf + s_pm[r3][tid]);
-    } else if (tid >= B && tid - B < nb) {
-      if (temporal) cp_async8(&s_t[b2][tid - B], temporal + s_pm[r3][tid - B]);
-    }
-  };
-  // work unit t < 6 B = (entry j, dimension i, half hh), strided over the CTA:
-  // tile-aligned weights of 4 cells
-  auto weights = [&](int bi) {
-    for (int t = tid; t < 6 * B; t += 256) {
-      const int pair = t >> 1, hh = t & 1;
-      const int j = pair / 3, i = pair - 3 * j;
-      if (j >= batch_len(bi)) continue;
-      const float4 c4 = s_c[bi % 3][j];
-      const float u = i == 0 ? c4.x : (i == 1 ? c4.y : c4.z);
-      const float r = sel3(kb.radius, i), ir = sel3(kb.inv_radius, i);
-      const int n = sel3(gp->nos, i), size = sel3(f.size, i);
-      const int lo = (int)ceilf(__fsub_rn(u, r));
-      int st = wrap_once(lo, n) - sel3(f.org, i);
-      if (st >= size) st -= n;  // footprint wraps into this tile from the end
-      float w[4];
-#pragma unroll
-      for (int l = 0; l < 4; ++l) {
-        const int cell = 4 * hh + l;
-        const int q = cell - st;
-        const float adx = fabsf(__fsub_rn((float)(lo + q), u));
-        w[l] = (q >= 0 && q < K && cell < size && adx <= r) ? kb_tap_fast(adx, ir, kb) : 0.f;
-      }
-      const int b2 = bi & 1;
-      if (i == 0) {
-        s_wx[b2][j][hh] = make_float4(w[0] * scale, w[1] * scale, w[2] * scale, w[3] * scale);
-      } else if (i == 1) {
-        s_wy[b2][j][hh] = make_float4(w[0], w[1], w[2], w[3]);
-      } else {
-        s_wz[b2][j][2 * hh] = make_float4(w[0], w[0], w[1], w[1]);
-        s_wz[b2][j][2 * hh + 1] = make_float4(w[2], w[2], w[3], w[3]);
-      }
-    }
-  };
-
-  float2 acc[8][4];
-#pragma unroll
-  for (int a = 0; a < 8; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = make_float2(0.f, 0.f);
-
-  copy_coords(0);
-  copy_coords(1);
-  cp_async_commit();
-  cp_async_wait<0>();
-  __syncthreads();
-  copy_values(0);
-  cp_async_commit();
-  copy_coords(2);
-  cp_async_commit();
-  weights(0);
-  const float* wxw = reinterpret_cast<const float*>(s_wx);
-  for (int bi = 0; bi < nbatch; ++bi) {
-    cp_async_wait<1>();  // values of bi and coordinates of bi + 1 have landed (this thread's)
-    __syncthreads();     // ... everyone's; weights of bi visible; buffers of bi - 1 free
-    copy_values(bi + 1);
-    cp_async_commit();
-    copy_coords(bi + 3);
-    cp_async_commit();
-    weights(bi + 1);
-    const int b2 = bi & 1, nb = batch_len(bi);
-#pragma unroll 1
-    for (int h32 = 0; h32 < B; h32 += 32) {
-      // entries whose footprint meets this warp's x-plane: one ballot per 32 entries
-      unsigned act = __ballot_sync(0xffffffffu, h32 + lane < nb && wxw[(b2 * B + h32 + lane) * 8 + warp] != 0.f);
-      while (act) {
-        const int j = h32 + __ffs(act) - 1;
-        act &= act - 1u;
-        const float wxv = wxw[(b2 * B + j) * 8 + warp];
-        const float4 wy0 = s_wy[b2][j][0], wy1 = s_wy[b2][j][1];
-        const float wy[8] = {wy0.x, wy0.y, wy0.z, wy0.w, wy1.x, wy1.y, wy1.z, wy1.w};
-        float2 wz[4];
-        {
-          const float4 c0 = s_wz[b2][j][2 * half], c1 = s_wz[b2][j][2 * half + 1];
-          wz[0] = make_float2(c0.x, c0.y);
-          wz[1] = make_float2(c0.z, c0.w);
-          wz[2] = make_float2(c1.x, c1.y);
-          wz[3] = make_float2(c1.z, c1.w);
-        }
-        float2 val = s_v[b2][j][coil];
-        if (dcf) {
-          const float d = s_d[b2][j];
-          val = make_float2(val.x * d, val.y * d);
-        }
-        if (temporal) {  // times conj(t)
-          const float2 t = s_t[b2][j];
-          val = make_float2(val.x * t.x + val.y * t.y, val.y * t.x - val.x * t.y);
-        }
-        val = make_float2(wxv * val.x, wxv * val.y);
-#pragma unroll
-        for (int a = 0; a < 8; ++a) {
-          if (wy[a] == 0.f) continue;  // uniform: the whole warp shares the rows
-          const float2 v2 = make_float2(wy[a] * val.x, wy[a] * val.y);
-#pragma unroll
-          for (int b = 0; b < 4; ++b) acc[a][b] = __ffma2_rn(wz[b], v2, acc[a][b]);
-        }
-      }
-    }
-  }
-  cp_async_wait<0>();
-
-  if (!has_coil || warp >= f.size[0]) return;
-  const int nos0 = gp->nos[0], nos1 = gp->nos[1], nos2 = gp->nos[2];
-  const int hs0 = layout == kInternal ? gp->hshift[0] : 0;
-  const int hs1 = layout == kInternal ? gp->hshift[1] : 0;
-  const int hs2 = layout == kInternal ? gp->hshift[2] : 0;
-  float2* dst = grid + (layout == kInternal ? gp->grid_off : gp->ugrid_off) + (int64_t)(c0 + coil) * gp->gos;
-  const int64_t xo = (int64_t)wrap_once(f.org[0] + warp - hs0, nos0) * nos1;
-  const int z0 = wrap_once(f.org[2] - hs2, nos2);
-#pragma unroll
-  for (int a = 0; a < 8; ++a) {
-    const int y = a;
-    if (y >= f.size[1]) break;
-    float2* rowp = dst + (xo + wrap_once(f.org[1] + y - hs1, nos1)) * nos2;
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      if (4 * half + b >= f.size[2]) break;
-      int z = z0 + 4 * half + b;
-      if (z >= nos2) z -= nos2;
-      if (it.split)
-        *split_slot(so, it.split, c0 + coil, (warp * f.size[1] + y) * f.size[2] + 4 * half + b) = acc[a][b];
-      else
-        rowp[z] = acc[a][b];
     }
   }
 }
@@ -1556,32 +1309,6 @@ int launch_grid_reg(mrn_plan* P, const float2* ksp, const float* dcf, const floa
   else { MRN_REG_SUB(8); }
 #undef MRN_REG_SUB
 #undef MRN_REG_LAUNCH
-  cudaError_t e = cudaGetLastError();
-  return e == cudaSuccess ? MRN_OK : cuda_fail(e);
-}
-
-bool grid_reg3_ok(const mrn_plan* P) {
-  return P->reg_grid && P->ndim == 3 && P->tmax_gcells[0] <= kReg3Tile &&
-         P->tmax_gcells[1] <= kReg3Tile && P->tmax_gcells[2] <= kReg3Tile;
-}
-
-int launch_grid_reg3(mrn_plan* P, const float2* ksp, const float* dcf, const float2* temporal,
-                     int layout, float2* grid, float scale, cudaStream_t st) {
-  if (P->n_items_grid == 0) return MRN_OK;
-  int cg = P->coil_group_req > 0 ? std::min(P->coil_group_req, P->max_coil) : P->max_coil;
-  cg = std::max(1, std::min(cg, kReg3Coils));
-  const int ng = (P->max_coil + cg - 1) / cg;
-  cg = (P->max_coil + ng - 1) / ng;
-  const dim3 gdim((unsigned)P->n_items_grid, (unsigned)ng);
-  const int K = P->kb.ntaps[0];
-#define MRN_REG3_LAUNCH(KK)                                                                       \
-  k_grid_reg3<KK><<<gdim, 256, 0, st>>>(P->d_items_g, P->d_slices, P->kb, P->d_coord_g, P->d_perm_g, \
-                                        ksp, dcf, temporal, grid, layout, scale, cg, split_out(P))
-  if (K == 5) MRN_REG3_LAUNCH(5);
-  else if (K == 6) MRN_REG3_LAUNCH(6);
-  else if (K == 7) MRN_REG3_LAUNCH(7);
-  else MRN_REG3_LAUNCH(8);
-#undef MRN_REG3_LAUNCH
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? MRN_OK : cuda_fail(e);
 }

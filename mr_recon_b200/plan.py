@@ -168,16 +168,14 @@ class Plan:
         self._call("mrn_sense_normal", ptr(x), ptr(mps), ptr(dcf), ptr(out), float(out_scale),
                    float(lam), ptr(pap), int(pap_stride))
 
-    def cg_init(self, b, Ab, x, r, p, p32, state, tol):
-        """x, r, p complex128; b, Ab, p32 complex64 (see mrn_cg_init)."""
-        self._call("mrn_cg_init", ptr(b), ptr(Ab), ptr(x), ptr(r), ptr(p), ptr(p32), ptr(state), float(tol))
+    def cg_init(self, b, Ab, x, r, p, state, tol):
+        self._call("mrn_cg_init", ptr(b), ptr(Ab), ptr(x), ptr(r), ptr(p), ptr(state), float(tol))
 
-    def cg_step(self, x, r, p, Ap, state, x32=None):
-        self._call("mrn_cg_step", ptr(x), ptr(r), ptr(p), ptr(Ap), ptr(x32) if x32 is not None else None,
-                   ptr(state))
+    def cg_step(self, x, r, p, Ap, state):
+        self._call("mrn_cg_step", ptr(x), ptr(r), ptr(p), ptr(Ap), ptr(state))
 
-    def cg_dir(self, r, p, p32, state):
-        self._call("mrn_cg_dir", ptr(r), ptr(p), ptr(p32), ptr(state))
+    def cg_dir(self, r, p, state):
+        self._call("mrn_cg_dir", ptr(r), ptr(p), ptr(state))
 
     def cg_dot(self, a, b, out):
         self._call("mrn_cg_dot", ptr(a), ptr(b), ptr(out))

@@ -51,6 +51,10 @@ except Exception:  # pragma: no cover
 F32 = np.float32
 C64 = np.complex64
 FFT_WORKERS = 1
+# False: FFTs in the input's precision (complex64, as the reference's torch.fft);
+# True: FFTs in complex128, so the only float32 rounding left in the NUFFT is
+# that of its stage outputs (used for the float64 CG-SENSE reference solution).
+FFT_DOUBLE = False
 
 
 def default_beta(width: float, oversamp: float) -> float:
@@ -269,6 +273,8 @@ def resize(x, oshape):
 def fft_c(x, axes, norm=None):
     """fft(): ifftshift -> fftn -> fftshift (fourier.py:37-48)."""
     y = np.fft.ifftshift(x, axes=axes)
+    if FFT_DOUBLE:
+        y = y.astype(np.complex128)
     y = _fftn(y, axes, FFT_WORKERS)
     if norm == "ortho":
         y = y / np.sqrt(np.prod([x.shape[a] for a in axes]))
@@ -279,6 +285,8 @@ def ifft_c(x, axes, norm=None):
     """ifft(): ifftshift -> ifftn -> fftshift (fourier.py:50-61); norm=None
     includes the 1/prod(N) factor."""
     y = np.fft.ifftshift(x, axes=axes)
+    if FFT_DOUBLE:
+        y = y.astype(np.complex128)
     y = _ifftn(y, axes, FFT_WORKERS)
     if norm == "ortho":
         y = y * np.sqrt(np.prod([x.shape[a] for a in axes]))

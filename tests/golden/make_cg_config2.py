@@ -10,7 +10,12 @@ eigenvalue of A^H A by 12 power iterations (seed 7) x 1.01, lambda 1e-3,
 
 Stores the oracle's solution with float64 iterates (``x_cg64``), the max
 eigenvalue used, and the distance of the reference's own float32 arithmetic
-(``conjugate_gradient_f32``) from that solution. Runs on the CPU in about a
+(``conjugate_gradient_f32``) from that solution. The oracle's FFTs run in
+complex128 here (``FFT_DOUBLE``), so its operator carries only the complex64
+rounding of each stage's output: a 20-iteration CG at lambda 1e-3 amplifies
+rounding that differs from one operator application to the next by about
+three orders of magnitude, so the reference solution must not carry more of
+it than necessary. Runs on the CPU in about a
 quarter of an hour (8 threads); no reference code is needed:
 
     python tests/golden/make_cg_config2.py
@@ -42,6 +47,7 @@ def problem():
 
 def main():
     O.FFT_WORKERS = 1
+    O.FFT_DOUBLE = True
     x, mps, trj = problem()
     nf = O.KBNufftOracle(IM, 1.25, 6)
     pool = ThreadPoolExecutor(os.cpu_count() or 1)

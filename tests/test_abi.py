@@ -75,8 +75,8 @@ def test_null_plan_calls_fail_cleanly():
     assert lib.mrn_plan_destroy(None) == _lib.MRN_OK
     betas = (C.c_double * 3)(8.0, 7.0, 6.0)
     assert lib.mrn_plan_set_beta(None, betas) == _lib.MRN_ERR_ARG
-    assert lib.mrn_cg_step(None, None, None, None, None, None, None, None) == _lib.MRN_ERR_ARG
-    assert lib.mrn_cg_dir(None, None, None, None, None, None) == _lib.MRN_ERR_ARG
+    assert lib.mrn_cg_step(None, None, None, None, None, None, None) == _lib.MRN_ERR_ARG
+    assert lib.mrn_cg_dir(None, None, None, None, None) == _lib.MRN_ERR_ARG
 
 
 def test_per_axis_beta_arguments_on_host():
