@@ -284,6 +284,7 @@ struct mrn_plan {
   int nslices = 0;
   int flags = 0;
   int device = 0;
+  int sm_count = 148;  // SMs of the plan's device
   double oversamp = 1.0;
   double width[mrn::kMaxDim] = {1, 1, 1};
   double beta = 0.0;

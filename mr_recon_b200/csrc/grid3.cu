@@ -206,27 +206,28 @@ k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
   }
   cp_async_wait<0>();
 
-  if (!has_coil || plane >= f.size[0]) return;
-  const int nos0 = gp->nos[0], nos1 = gp->nos[1], nos2 = gp->nos[2];
-  const int hs0 = layout == kInternal ? gp->hshift[0] : 0;
-  const int hs1 = layout == kInternal ? gp->hshift[1] : 0;
-  const int hs2 = layout == kInternal ? gp->hshift[2] : 0;
-  float2* dst = grid + (layout == kInternal ? gp->grid_off : gp->ugrid_off) + (int64_t)(c0 + coil) * gp->gos;
-  const int64_t xo = (int64_t)wrap_once(f.org[0] + plane - hs0, nos0) * nos1;
-  const int zs = wrap_once(f.org[2] - hs2, nos2);
+  if (has_coil && plane < f.size[0]) {
+    const int nos0 = gp->nos[0], nos1 = gp->nos[1], nos2 = gp->nos[2];
+    const int hs0 = layout == kInternal ? gp->hshift[0] : 0;
+    const int hs1 = layout == kInternal ? gp->hshift[1] : 0;
+    const int hs2 = layout == kInternal ? gp->hshift[2] : 0;
+    float2* dst = grid + (layout == kInternal ? gp->grid_off : gp->ugrid_off) + (int64_t)(c0 + coil) * gp->gos;
+    const int64_t xo = (int64_t)wrap_once(f.org[0] + plane - hs0, nos0) * nos1;
+    const int zs = wrap_once(f.org[2] - hs2, nos2);
 #pragma unroll
-  for (int y = 0; y < T; ++y) {
-    if (y >= f.size[1]) break;
-    float2* rowp = dst + (xo + wrap_once(f.org[1] + y - hs1, nos1)) * nos2;
+    for (int y = 0; y < T; ++y) {
+      if (y >= f.size[1]) break;
+      float2* rowp = dst + (xo + wrap_once(f.org[1] + y - hs1, nos1)) * nos2;
 #pragma unroll
-    for (int z = 0; z < T; ++z) {
-      if (z >= f.size[2]) break;
-      int zz = zs + z;
-      if (zz >= nos2) zz -= nos2;
-      if (it.split)
-        *split_slot(so, it.split, c0 + coil, (plane * f.size[1] + y) * f.size[2] + z) = acc[y][z];
-      else
-        rowp[zz] = acc[y][z];
+      for (int z = 0; z < T; ++z) {
+        if (z >= f.size[2]) break;
+        int zz = zs + z;
+        if (zz >= nos2) zz -= nos2;
+        if (it.split)
+          *split_slot(so, it.split, c0 + coil, (plane * f.size[1] + y) * f.size[2] + z) = acc[y][z];
+        else
+          rowp[zz] = acc[y][z];
+      }
     }
   }
 }

@@ -204,11 +204,13 @@ __global__ void k_emit_items(const SliceGeom* __restrict__ sl, int ns, const int
     split_tiles[k] = make_int4(t, base, n, 0);
   }
   for (int q = 0; q < n; ++q) {
+    // the tile's entries spread evenly over its items (at most chunk each)
+    const int b0 = (int)(((int64_t)q * c) / n), b1 = (int)(((int64_t)(q + 1) * c) / n);
     Item it;
     it.slice = s;
     it.tile = t - (gridding ? sl[s].gtile_base : sl[s].tile_base);
-    it.start = start[t] + q * chunk;
-    it.count = max(0, min(chunk, c - q * chunk));
+    it.start = start[t] + b0;
+    it.count = b1 - b0;
     it.split = base >= 0 ? base + q + 1 : 0;
     it.pad[0] = it.pad[1] = it.pad[2] = 0;
     items[ioff[t] + q] = it;
@@ -603,6 +605,7 @@ int mrn_plan_create(mrn_plan** out, int ndim, int n_slices, const int* im_size,
 
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) { delete P; return cuda_fail(e); }
+  cudaDeviceGetAttribute(&P->sm_count, cudaDevAttrMultiProcessorCount, device);
 
   int rc = MRN_OK;
 #define PK(x) do { rc = (x); if (rc != MRN_OK) { mrn_plan_destroy(P); return rc; } } while (0)

@@ -18,7 +18,7 @@
 //     written back once with plain coalesced stores -- no global atomics and
 //     no zero fill of the output. Tiles so dense that they were split over
 //     several CTAs get one partial tile per CTA, summed in item order by a
-//     reduction pass, so every gridding path gives the same bits run to run.
+//     reduction pass, so a tile's parts add in the same order on every run.
 // Tap selection and weights follow the reference exactly: taps j = lo + q,
 // lo = ceil(u - W/2), valid iff |(float)j - u| <= W/2 (kernels.py:268-393),
 // weight = prod_d KB(|j_d - u_d| / (W_d/2)) (norm '1'), cells wrap circularly.
@@ -26,13 +26,11 @@
 
 #include "common.cuh"
 #include "internal.cuh"
+#include "tile_util.cuh"
 
 namespace mrn {
 
-struct TileFrame {
-  int org[kMaxDim];   // first centred cell of the tile
-  int size[kMaxDim];  // tile cells per dim
-};
+using TileFrame = Frame;
 
 __device__ __forceinline__ TileFrame tile_frame(const SliceGeom& g, int tile, int D,
                                                 bool gridding = false) {
@@ -449,51 +447,65 @@ k_grid(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBParam
 }
 
 // Sum the partial tiles of every split gridding tile in item order and store
-// the result: one CTA per (split tile, group of kSplitCoils coils), threads
-// over (coil, cell), each thread adding the tile's slots first to last. The
-// gridding kernels ran before on the same stream and wrote every slot read
-// here (a split tile's items are slots base .. base + n - 1).
+// the result. Work units are (split tile, group of kSplitCoils coils); a
+// grid of a few CTAs per SM strides over them (the number of split tiles is
+// known only on the device, counts[3]), threads over (coil, cell), each
+// thread adding the tile's slots first to last with four loads in flight.
+// The gridding kernel ran before on the same stream and wrote every slot
+// read here (a split tile's items are slots base .. base + n - 1).
 constexpr int kSplitCoils = 8;
 
 template <int D>
 __global__ void __launch_bounds__(256)
 k_reduce_split(const int4* __restrict__ split_tiles, const int* __restrict__ counts,
-               const SliceGeom* __restrict__ sl, int ns, SplitOut so, float2* __restrict__ grid,
-               int layout) {
-  if ((int)blockIdx.x >= counts[3]) return;
-  const int4 sp = split_tiles[blockIdx.x];
-  const int t = sp.x, base = sp.y, nparts = sp.z;
-  int s = 0;
-  {
-    int lo = 0, hi = ns - 1;
-    while (lo < hi) {
-      int mid = (lo + hi + 1) >> 1;
-      if (sl[mid].gtile_base <= t) lo = mid; else hi = mid - 1;
+               const SliceGeom* __restrict__ sl, int ns, int coil_groups, SplitOut so,
+               float2* __restrict__ grid, int layout) {
+  const int units = counts[3] * coil_groups;
+  for (int unit = blockIdx.x; unit < units; unit += gridDim.x) {
+    const int4 sp = split_tiles[unit / coil_groups];
+    const int t = sp.x, base = sp.y, nparts = sp.z;
+    int s = 0;
+    {
+      int lo = 0, hi = ns - 1;
+      while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (sl[mid].gtile_base <= t) lo = mid; else hi = mid - 1;
+      }
+      s = lo;
     }
-    s = lo;
-  }
-  const SliceGeom& g = sl[s];
-  const TileFrame f = tile_frame(g, t - g.gtile_base, D, true);
-  int hs[kMaxDim];
-  for (int i = 0; i < kMaxDim; ++i) hs[i] = (i < D && layout == kInternal) ? g.hshift[i] : 0;
-  int cells = 1;
-  for (int i = 0; i < D; ++i) cells *= f.size[i];
-  const int cbeg = blockIdx.y * kSplitCoils;
-  const int ncl = min(kSplitCoils, g.ncoil - cbeg);
-  if (ncl <= 0) return;
-  const int64_t goff = (layout == kInternal ? g.grid_off : g.ugrid_off) + (int64_t)cbeg * g.gos;
-  for (int idx = threadIdx.x; idx < ncl * cells; idx += blockDim.x) {
-    const int c = idx / cells, cell = idx - c * cells;
-    const float2* src = split_slot(so, base + 1, cbeg + c, cell);
-    float2 acc = src[0];
-    for (int q = 1; q < nparts; ++q) {
-      const float2 v = src[(int64_t)q * so.slot_stride];
-      acc.x += v.x;
-      acc.y += v.y;
+    const SliceGeom& g = sl[s];
+    const TileFrame f = tile_frame(g, t - g.gtile_base, D, true);
+    int hs[kMaxDim];
+    for (int i = 0; i < kMaxDim; ++i) hs[i] = (i < D && layout == kInternal) ? g.hshift[i] : 0;
+    int cells = 1;
+    for (int i = 0; i < D; ++i) cells *= f.size[i];
+    const int cbeg = (unit % coil_groups) * kSplitCoils;
+    const int ncl = min(kSplitCoils, g.ncoil - cbeg);
+    const int64_t goff = (layout == kInternal ? g.grid_off : g.ugrid_off) + (int64_t)cbeg * g.gos;
+    for (int idx = threadIdx.x; idx < ncl * cells; idx += blockDim.x) {
+      const int c = idx / cells, cell = idx - c * cells;
+      const float2* src = split_slot(so, base + 1, cbeg + c, cell);
+      float2 acc = make_float2(0.f, 0.f);
+      int q = 0;
+      for (; q + 4 <= nparts; q += 4) {
+        float2 v[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[k] = src[(int64_t)(q + k) * so.slot_stride];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          acc.x += v[k].x;
+          acc.y += v[k].y;
+        }
+      }
+      for (; q < nparts; ++q) {
+        const float2 v = src[(int64_t)q * so.slot_stride];
+        acc.x += v.x;
+        acc.y += v.y;
+      }
+      int64_t lin;
+      tile_storage<D>(g, f, hs, cell, &lin);
+      grid[goff + (int64_t)c * g.gos + lin] = acc;
     }
-    int64_t lin;
-    tile_storage<D>(g, f, hs, cell, &lin);
-    grid[goff + (int64_t)c * g.gos + lin] = acc;
   }
 }
 
@@ -787,14 +799,16 @@ int launch_grid(mrn_plan* P, const float2* ksp, const float* dcf, GridLayout lay
 
 static int launch_reduce_split(mrn_plan* P, GridLayout layout, float2* grid, cudaStream_t st) {
   if (P->n_split == 0) return MRN_OK;
-  const dim3 nb((unsigned)P->n_split, (unsigned)((P->max_coil + kSplitCoils - 1) / kSplitCoils));
+  const int groups = (P->max_coil + kSplitCoils - 1) / kSplitCoils;
+  const int64_t units = P->n_split * groups;
+  const unsigned nb = (unsigned)std::max<int64_t>(1, std::min<int64_t>(units, 4 * (int64_t)P->sm_count));
   const SplitOut so = split_out(P);
   if (P->ndim == 1)
-    k_reduce_split<1><<<nb, 256, 0, st>>>(P->d_split_tiles, P->d_counts, P->d_slices, P->nslices, so, grid, (int)layout);
+    k_reduce_split<1><<<nb, 256, 0, st>>>(P->d_split_tiles, P->d_counts, P->d_slices, P->nslices, groups, so, grid, (int)layout);
   else if (P->ndim == 2)
-    k_reduce_split<2><<<nb, 256, 0, st>>>(P->d_split_tiles, P->d_counts, P->d_slices, P->nslices, so, grid, (int)layout);
+    k_reduce_split<2><<<nb, 256, 0, st>>>(P->d_split_tiles, P->d_counts, P->d_slices, P->nslices, groups, so, grid, (int)layout);
   else
-    k_reduce_split<3><<<nb, 256, 0, st>>>(P->d_split_tiles, P->d_counts, P->d_slices, P->nslices, so, grid, (int)layout);
+    k_reduce_split<3><<<nb, 256, 0, st>>>(P->d_split_tiles, P->d_counts, P->d_slices, P->nslices, groups, so, grid, (int)layout);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? MRN_OK : cuda_fail(e);
 }

@@ -1062,24 +1062,25 @@ k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBP
           acc[a][b].y += __shfl_xor_sync(0xffffffffu, acc[a][b].y, o);
         }
   }
-  if (!has_coil || sub != 0) return;
-  const int hs0 = layout == kInternal ? gp->hshift[0] : 0;
-  const int hs1 = layout == kInternal ? gp->hshift[1] : 0;
-  const int64_t gos = gp->gos;
-  float2* dst = grid + (layout == kInternal ? gp->grid_off : gp->ugrid_off) + (int64_t)(c0 + coil) * gos;
-  const int s1 = wrap_once(f.org[1] - hs1, nos1);
+  if (has_coil && sub == 0) {
+    const int hs0 = layout == kInternal ? gp->hshift[0] : 0;
+    const int hs1 = layout == kInternal ? gp->hshift[1] : 0;
+    const int64_t gos = gp->gos;
+    float2* dst = grid + (layout == kInternal ? gp->grid_off : gp->ugrid_off) + (int64_t)(c0 + coil) * gos;
+    const int s1 = wrap_once(f.org[1] - hs1, nos1);
 #pragma unroll
-  for (int a = 0; a < R; ++a) {
-    const int row = warp * R + a;
-    if (row >= f.size[0]) break;
-    const int64_t rowo = (int64_t)wrap_once(f.org[0] + row - hs0, nos0) * nos1;
+    for (int a = 0; a < R; ++a) {
+      const int row = warp * R + a;
+      if (row >= f.size[0]) break;
+      const int64_t rowo = (int64_t)wrap_once(f.org[0] + row - hs0, nos0) * nos1;
 #pragma unroll
-    for (int b = 0; b < T; ++b) {
-      if (b >= f.size[1]) break;
-      int s = s1 + b;
-      if (s >= nos1) s -= nos1;
-      if (it.split) *split_slot(so, it.split, c0 + coil, row * f.size[1] + b) = acc[a][b];
-      else dst[rowo + s] = acc[a][b];
+      for (int b = 0; b < T; ++b) {
+        if (b >= f.size[1]) break;
+        int s = s1 + b;
+        if (s >= nos1) s -= nos1;
+        if (it.split) *split_slot(so, it.split, c0 + coil, row * f.size[1] + b) = acc[a][b];
+        else dst[rowo + s] = acc[a][b];
+      }
     }
   }
 }

@@ -16,6 +16,7 @@
 
 #include "common.cuh"
 #include "internal.cuh"
+#include "tile_util.cuh"
 
 namespace mrn {
 
