@@ -203,6 +203,30 @@ int mrn_sense_normal(mrn_plan* plan, const void* x, const void* mps, const float
                      void* stream);
 
 /*
+ * Toeplitz (FFT-only) normal operator A^H A, for plans without MRN_PLAN_RAW.
+ * Replaces NUFFT.normal_toeplitz (fourier.py:302-352) and the Toeplitz branch
+ * of sense_linop.normal (linops.py:1249-1308) for one image per slice and no
+ * time segmentation. The kernel is what calc_teoplitz_kernels
+ * (fourier.py:552-582) returns: per slice the centred complex64 kernel on the
+ * padded grid pad_size[s * ndim + i] (normally twice the image size; pad_size
+ * - im_size must be even, the centred pad of PadLast), slices back to back.
+ * mrn_plan_set_toeplitz copies it into the plan (reordered for the FFT, with
+ * the 1 / prod(pad) of the two orthonormal FFTs folded in), allocating the
+ * padded grids and their cuFFT plans when the sizes change; it needs no
+ * trajectory. Then, with centred orthonormal FFTs on the padded grid:
+ *   mrn_toeplitz_normal      : out[c] = crop(IFFT(K * FFT(pad(img[c]))))
+ *                              (img/out in the image layout [C][N...])
+ *   mrn_sense_normal_toeplitz: out = out_scale * sum_c conj(mps[c])
+ *                              crop(IFFT(K * FFT(pad(mps[c] x)))) + lam x,
+ *                              pap as in mrn_sense_normal (fixed-order sum)
+ * Both return MRN_ERR_STATE before mrn_plan_set_toeplitz.
+ */
+int mrn_plan_set_toeplitz(mrn_plan* plan, const int* pad_size, const void* kern, void* stream);
+int mrn_toeplitz_normal(mrn_plan* plan, const void* img, void* out, void* stream);
+int mrn_sense_normal_toeplitz(mrn_plan* plan, const void* x, const void* mps, void* out, float out_scale,
+                              float lam, double* pap, int pap_stride, void* stream);
+
+/*
  * Conjugate-gradient vector steps for n_slices independent systems (the loop
  * body of conjugate_gradient, algs.py:779-872), complex64 vectors with
  * float64 dot products and norms. Every float64 sum is taken in a fixed order

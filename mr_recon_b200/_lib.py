@@ -71,6 +71,9 @@ SIGNATURES = {
     "mrn_sense_forward": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "mrn_sense_adjoint": (_i, [_vp, _vp, _vp, _vp, _vp, _f, _vp]),
     "mrn_sense_normal": (_i, [_vp, _vp, _vp, _vp, _vp, _f, _f, _vp, _i, _vp]),
+    "mrn_plan_set_toeplitz": (_i, [_vp, _pi, _vp, _vp]),
+    "mrn_toeplitz_normal": (_i, [_vp, _vp, _vp, _vp]),
+    "mrn_sense_normal_toeplitz": (_i, [_vp, _vp, _vp, _vp, _f, _f, _vp, _i, _vp]),
     "mrn_cg_init": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _d, _vp]),
     "mrn_cg_step": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "mrn_cg_dir": (_i, [_vp, _vp, _vp, _vp, _vp]),

@@ -166,8 +166,12 @@ class SenseCG:
     """
 
     def __init__(self, plan, mps: torch.Tensor, dcf: Optional[torch.Tensor], max_iter: int,
-                 lamda_l2: float, max_eigen, tolerance: float = 1e-8):
+                 lamda_l2: float, max_eigen, tolerance: float = 1e-8, toeplitz: bool = False):
         self.plan = plan
+        # normal operator: the Toeplitz one bound to the plan (FFT-only), or the NUFFT's
+        self.toeplitz = bool(toeplitz)
+        if self.toeplitz and getattr(plan, "toeplitz_pad", None) is None:
+            raise ValueError("SenseCG(toeplitz=True) needs Toeplitz kernels bound to the plan")
         self.mps = mps
         self.dcf = dcf
         self.max_iter = int(max_iter)
@@ -194,11 +198,15 @@ class SenseCG:
         if self.max_iter == 0:
             self.x.copy_(self.b)
             return
-        pl.sense_normal(self.b, self.mps, self.dcf, self.Ap, s_nrm, self.lam)
+        if self.toeplitz:
+            normal = lambda v, out, *a: pl.sense_normal_toeplitz(v, self.mps, out, *a)  # noqa: E731
+        else:
+            normal = lambda v, out, *a: pl.sense_normal(v, self.mps, self.dcf, out, *a)  # noqa: E731
+        normal(self.b, self.Ap, s_nrm, self.lam)
         pl.cg_init(self.b, self.Ap, self.x, self.r, self.p, self.state, self.tol)
         pap = self.state[1:]
         for _ in range(self.max_iter):
-            pl.sense_normal(self.p, self.mps, self.dcf, self.Ap, s_nrm, self.lam, pap, 8)
+            normal(self.p, self.Ap, s_nrm, self.lam, pap, 8)
             pl.cg_step(self.x, self.r, self.p, self.Ap, self.state)
             pl.cg_dir(self.r, self.p, self.state)
 

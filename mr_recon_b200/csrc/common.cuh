@@ -365,6 +365,7 @@ struct mrn_plan {
   size_t cub_tmp_bytes = 0;
   float2* d_grid = nullptr;         // internal oversampled grid (natural order, grouped)
   float2* d_ksp_tmp = nullptr;      // sample scratch for normal operators
+  void* toep = nullptr;             // Toeplitz normal operator state (toeplitz.cu), or null
   unsigned* d_sync = nullptr;       // last-block counters: [0] k_cg_dir, [1] CG sums, [2] k_post
   double* d_red = nullptr;          // CG block partial sums, [n_slices][kMaxRedBlocks]
   double* d_rowpart = nullptr;      // k_post per-row partials of Re<x, out>, [n_xrow]

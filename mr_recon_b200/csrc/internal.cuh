@@ -88,4 +88,7 @@ int launch_post(mrn_plan* P, PostMode mode, const float2* mps, float2* out, floa
 int launch_shift_copy(mrn_plan* P, const float2* src, float2* dst, int to_user, cudaStream_t st);
 int run_fft(mrn_plan* P, int direction, cudaStream_t st);
 
+// Toeplitz normal operator state (toeplitz.cu)
+void toep_free(mrn_plan* P);
+
 }  // namespace mrn

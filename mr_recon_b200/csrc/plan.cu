@@ -741,6 +741,7 @@ int mrn_plan_destroy(mrn_plan* P) {
     if (e) cudaEventDestroy(e);
   for (auto& fg : P->fft)
     if (fg.handle) cufftDestroy(fg.handle);
+  toep_free(P);
   void* bufs[] = {P->d_slices, P->d_apod, P->d_coord_i, P->d_perm_i, P->d_coord_g, P->d_perm_g,
                   P->d_key_a, P->d_key_b, P->d_key_is, P->d_key_g, P->d_val_a, P->d_val_b, P->d_coord_tmp,
                   P->d_entry_cnt, P->d_tile_start_i, P->d_tile_end_i, P->d_tile_start_g,

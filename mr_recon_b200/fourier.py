@@ -322,6 +322,34 @@ class b200_nufft(NUFFT):
         plan.adjoint_ift(ksp_os.detach().to(complex_dtype).contiguous(), out)
         return out
 
+    def normal_toeplitz(self, img: torch.Tensor, toeplitz_kernels: torch.Tensor) -> torch.Tensor:
+        """FFT-only normal operator with precomputed kernels (fourier.py:302-352):
+        centred pad, orthonormal FFT, x kernel, inverse FFT and crop in one plan
+        call (mrn_toeplitz_normal). img (N, *B, *im), kernels (N, *im_os)."""
+        _lib.require_cuda(img, "image")
+        d = len(self.im_size)
+        N = img.shape[0]
+        bshape = tuple(img.shape[1:-d])
+        if tuple(img.shape[-d:]) != tuple(self.im_size):
+            raise ValueError(f"image size {tuple(img.shape[-d:])} != {tuple(self.im_size)}")
+        im_os = tuple(int(v) for v in toeplitz_kernels.shape[-d:])
+        if toeplitz_kernels.shape[0] != N:
+            raise ValueError("one Toeplitz kernel per batch element is needed")
+        C = int(np.prod(bshape)) if bshape else 1
+        key = ("toeplitz", N, C, im_os, str(img.device))
+
+        def make():
+            return Plan([tuple(self.im_size)] * N, [0] * N, [C] * N, self.oversamp, self._widths(), self.beta,
+                        apodize=self.apodize, device=img.device)
+
+        plan = self._plans.get(key, None, make)
+        # the kernels are copied into the plan on every call (a reorder pass the
+        # size of one kernel per slice), so a caller's new kernels are never missed
+        plan.set_toeplitz(toeplitz_kernels, [im_os] * N)
+        out = torch.empty((N, *bshape, *self.im_size), dtype=complex_dtype, device=img.device)
+        plan.toeplitz_normal(img.detach().to(complex_dtype).contiguous(), out)
+        return out
+
     def calc_teoplitz_kernels(self, trj: torch.Tensor, weights: Optional[torch.Tensor] = None,
                               os_factor: Optional[float] = 2.0):
         """Toeplitz kernels (fourier.py:552-582)."""

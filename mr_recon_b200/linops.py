@@ -290,6 +290,9 @@ class sense_linop(linop):
                 kerns.append(nufft.calc_teoplitz_kernels(trj[None,], weights[b1:b2])[0])
             L = temporal_funcs.shape[0]
             self.toep_kerns = rearrange(torch.stack(kerns, dim=0), "(n1 n2) ... -> n1 n2 ...", n1=L, n2=L)
+            if self.plan is not None and L == 1:
+                # one image, no segments: the fused Toeplitz normal (mrn_sense_normal_toeplitz)
+                self.plan.set_toeplitz(self.toep_kerns[0, 0], [tuple(self.toep_kerns.shape[-len(im_size):])])
         else:
             self.toep_kerns = None
 
@@ -397,6 +400,11 @@ class sense_linop(linop):
                 self.plan.sense_normal(x, self.mps, self.dcf, out)
                 return out
             return self.adjoint(self.forward(img))
+        if self.plan is not None and getattr(self.plan, "toeplitz_pad", None) is not None:
+            x = img.to(complex_dtype).contiguous()
+            out = torch.empty_like(x)
+            self.plan.sense_normal_toeplitz(x, self.mps, out)
+            return out
         L = self.temporal_funcs.shape[0]
         dim = len(self.im_size)
         im_size_os = self.toep_kerns.shape[-dim:]

@@ -168,6 +168,27 @@ class Plan:
         self._call("mrn_sense_normal", ptr(x), ptr(mps), ptr(dcf), ptr(out), float(out_scale),
                    float(lam), ptr(pap), int(pap_stride))
 
+    def set_toeplitz(self, kern: torch.Tensor, pad_sizes) -> None:
+        """Bind Toeplitz kernels (calc_teoplitz_kernels' output, per slice on
+        the padded grid pad_sizes[s], slices back to back); see mrn_plan_set_toeplitz."""
+        _lib.require_cuda(kern, "Toeplitz kernel")
+        k = kern.detach().to(torch.complex64).contiguous()
+        ps = [int(v) for s in pad_sizes for v in s]
+        if k.numel() != sum(int(torch.tensor(s).prod()) for s in pad_sizes):
+            raise ValueError("Toeplitz kernel size does not match the padded grids")
+        arr = (C.c_int * len(ps))(*ps)
+        with torch.cuda.device(self.device):
+            check(self.lib.mrn_plan_set_toeplitz(self.handle, arr, ptr(k), self.stream()),
+                  "mrn_plan_set_toeplitz")
+        self.toeplitz_pad = [tuple(s) for s in pad_sizes]
+
+    def toeplitz_normal(self, img, out):
+        self._call("mrn_toeplitz_normal", ptr(img), ptr(out))
+
+    def sense_normal_toeplitz(self, x, mps, out, out_scale=1.0, lam=0.0, pap=None, pap_stride=1):
+        self._call("mrn_sense_normal_toeplitz", ptr(x), ptr(mps), ptr(out), float(out_scale), float(lam),
+                   ptr(pap), int(pap_stride))
+
     def cg_init(self, b, Ab, x, r, p, state, tol):
         self._call("mrn_cg_init", ptr(b), ptr(Ab), ptr(x), ptr(r), ptr(p), ptr(state), float(tol))
 

@@ -28,12 +28,13 @@ def _fused_solver(A, max_iter, lamda_l2, max_eigen, tolerance, graph, ksp):
     on the linop, keyed by the settings and the identity of its plan, coil maps
     and density weights, so repeated calls (one per slice or frame) reuse the
     buffers and, with ``graph=True``, the CUDA graph captured on the first call."""
+    toep = bool(getattr(A, "use_toeplitz", False)) and getattr(A.plan, "toeplitz_pad", None) is not None
     key = (int(max_iter), float(lamda_l2), float(max_eigen), float(tolerance), bool(graph),
-           id(A.plan), id(A.mps), id(A.dcf))
+           id(A.plan), id(A.mps), id(A.dcf), toep)
     cache = A.__dict__.setdefault("_fused_cg", {})
     cg = cache.get(key)
     if cg is None:
-        cg = SenseCG(A.plan, A.mps, A.dcf, max_iter, lamda_l2, max_eigen, tolerance)
+        cg = SenseCG(A.plan, A.mps, A.dcf, max_iter, lamda_l2, max_eigen, tolerance, toeplitz=toep)
         if graph:
             cg.ksp.copy_(ksp.reshape(-1))
             cg.capture()
