@@ -16,8 +16,10 @@ solves/s (20 iterations, lambda 1e-3, graph-captured vs eager), the CPU
 oracle baseline, and SM clocks sampled during the timed region.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-Multi-GPU: launched by torchrun, one independent replica per rank (weak
-scaling, no data-path collective), time = max over ranks.
+Multi-GPU: one process per GPU (started by torchrun, or by this script with
+--gpus N); the headline workload runs one independent replica per rank (weak
+scaling, no data-path collective) and the batched configuration shards its
+64 slices over the ranks; job time = max over ranks.
 """
 
 from __future__ import annotations
@@ -251,27 +253,42 @@ def bench_c3(dev, steps, peak, N=192, spokes=20000):
     }
 
 
-def bench_c4(dev, iters=30, seed=4, n_slices=64):
+def bench_c4(dev, iters=30, seed=4, n_slices=64, world=1, rank=0):
     """Batched uneven CG-SENSE: 64 slices (matrix from {160..256}^2, 8-32
     coils, 10k-100k spiral samples), 30 iterations captured in one CUDA graph
     with autotuned bins/tiles, against a loop of per-slice solves on the same
     kernels. Per-slice eigenvalue normalisation (recons.py:117-123) is folded
-    into the coil maps: A_s / sqrt(l_s)."""
+    into the coil maps: A_s / sqrt(l_s). With several ranks the slices are
+    sharded by cost (coils x samples, shard_slices): each rank solves its own
+    range in one graph, the job time is the slowest rank's (no data-path
+    collective), and the per-slice loop is not run."""
     import torch
     from mr_recon_b200 import synth
     from mr_recon_b200.algs import SenseCG
     from mr_recon_b200.autotune import autotune
     from mr_recon_b200.plan import Plan
+    from mr_recon_b200.shard import max_over_ranks, shard_slices
     rng = np.random.RandomState(seed)
-    sizes = rng.choice([160, 192, 224, 256], n_slices)
-    coils = rng.randint(8, 33, n_slices)
-    npts = rng.randint(10000, 100001, n_slices) // 16 * 16
+    all_sizes = rng.choice([160, 192, 224, 256], n_slices)
+    all_coils = rng.randint(8, 33, n_slices)
+    all_npts = rng.randint(10000, 100001, n_slices) // 16 * 16
+    first, last = shard_slices([float(c) * float(m) for c, m in zip(all_coils, all_npts)], world, rank)
+    sizes, coils, npts = all_sizes[first:last], all_coils[first:last], all_npts[first:last]
     xs, mps, trjs = [], [], []
     for s in range(n_slices):
-        N = int(sizes[s])
-        xs.append(synth.ellipse_phantom((N, N), 20, rng).astype(np.complex64).reshape(-1))
-        mps.append(synth.gaussian_coil_maps((N, N), int(coils[s])).astype(np.complex64).reshape(-1))
-        trjs.append(synth.vd_spiral(16, int(npts[s]) // 16, N / 2.0).reshape(-1, 2))
+        N = int(all_sizes[s])
+        phantom = synth.ellipse_phantom((N, N), 20, rng)  # drawn for every slice: same data on any rank count
+        if not first <= s < last:
+            continue
+        xs.append(phantom.astype(np.complex64).reshape(-1))
+        mps.append(synth.gaussian_coil_maps((N, N), int(all_coils[s])).astype(np.complex64).reshape(-1))
+        trjs.append(synth.vd_spiral(16, int(all_npts[s]) // 16, N / 2.0).reshape(-1, 2))
+    mine = last - first
+    if mine == 0:  # more ranks than slices: this rank only joins the timing
+        b_ms = max_over_ranks(0.0, dev)
+        return {"slices_this_rank": 0, "ranks": world, "ms_per_batch_graph": b_ms,
+                "slice_solves_per_s_batched_graph": n_slices * 1e3 / b_ms}
+    n_mine = mine
     ims = [(int(n), int(n)) for n in sizes]
     x_t = torch.from_numpy(np.concatenate(xs)).to(dev)
     m_t = torch.from_numpy(np.concatenate(mps)).to(dev)
@@ -294,11 +311,11 @@ def bench_c4(dev, iters=30, seed=4, n_slices=64):
     lam = None
     for _ in range(15):
         plan.sense_normal(v, m_t, None, z)
-        lam = torch.stack([z[xoff[s]:xoff[s + 1]].norm() for s in range(n_slices)])
+        lam = torch.stack([z[xoff[s]:xoff[s + 1]].norm() for s in range(n_mine)])
         v = z / torch.repeat_interleave(lam, torch.tensor(np.diff(xoff), device=dev))
     lam = (lam * 1.01).double()
     m_s = m_t.clone()
-    for s in range(n_slices):
+    for s in range(n_mine):
         m_s[img_off[s]:img_off[s] + nimg[s]] /= float(lam[s].sqrt())
     solver = SenseCG(plan, m_s, None, iters, 1e-3, 1.0)
     solver.ksp.copy_(ksp)
@@ -313,7 +330,17 @@ def bench_c4(dev, iters=30, seed=4, n_slices=64):
         solver.graph.replay()
     e1.record()
     torch.cuda.synchronize()
-    b_ms = e0.elapsed_time(e1) / reps
+    b_ms = max_over_ranks(e0.elapsed_time(e1) / reps, dev)  # the slowest rank sets the job time
+    out = {
+        "workload": "batched uneven CG-SENSE: 64 slices, N in {160..256}^2, 8-32 coils, 10k-100k spiral "
+                    "samples, 30 iterations, lambda 1e-3",
+        "slice_solves_per_s_batched_graph": n_slices * 1e3 / b_ms, "ms_per_batch_graph": b_ms,
+        "ranks": world, "slices_this_rank": n_mine,
+        "autotune": {k: v for k, v in tune.items()}, "autotune_s": tune_s,
+        "total_coil_samples": int(sum(int(c) * int(m) for c, m in zip(all_coils, all_npts))),
+    }
+    if world > 1:
+        return out
     # per-slice loop on the same kernels: one plan and one eager solve per slice
     ksp_off = [int(o) for o in plan.ksp_off]
     singles = []
@@ -332,15 +359,9 @@ def bench_c4(dev, iters=30, seed=4, n_slices=64):
     torch.cuda.synchronize()
     l_ms = e0.elapsed_time(e1)
     xl = torch.cat(xs_loop)
-    return {
-        "workload": "batched uneven CG-SENSE: 64 slices, N in {160..256}^2, 8-32 coils, 10k-100k spiral "
-                    "samples, 30 iterations, lambda 1e-3",
-        "slice_solves_per_s_batched_graph": n_slices * 1e3 / b_ms, "ms_per_batch_graph": b_ms,
-        "slice_solves_per_s_per_slice_loop": n_slices * 1e3 / l_ms, "ms_per_slice_loop": l_ms,
-        "speedup": l_ms / b_ms, "batched_vs_loop_rel_diff": float((xb - xl).norm() / xl.norm()),
-        "autotune": {k: v for k, v in tune.items()}, "autotune_s": tune_s,
-        "total_coil_samples": int(sum(int(c) * int(m) for c, m in zip(coils, npts))),
-    }
+    out.update({"slice_solves_per_s_per_slice_loop": n_slices * 1e3 / l_ms, "ms_per_slice_loop": l_ms,
+                "speedup": l_ms / b_ms, "batched_vs_loop_rel_diff": float((xb - xl).norm() / xl.norm())})
+    return out
 
 
 def bench_c5(dev, iters=20, L=20):
@@ -464,6 +485,15 @@ def main():
                     help="comma list of the other configurations to add to the line: c3 (3D), c4 (batched "
                          "uneven CG), c5 (B0 segments); empty for none")
     args = ap.parse_args()
+    if args.impl == "ours" and args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: start the ranks here when no launcher did
+        import socket
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+               "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+        sys.exit(subprocess.call(cmd))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -715,12 +745,12 @@ def main():
             rel_err["cg_sense"] = cg["rel_err_vs_oracle_cg64"]
 
     extra = {}
-    if rank == 0 and world == 1:
-        want = [e.strip() for e in args.extra.split(",") if e.strip()]
+    want = [e.strip() for e in args.extra.split(",") if e.strip()]
+    if "c4" in want:  # every rank: the 64 slices are sharded over the ranks
+        extra["c4"] = bench_c4(dev, world=world, rank=rank)
+    if rank == 0:  # single-problem configurations on the first GPU
         if "c3" in want:
             extra["c3"] = bench_c3(dev, 5, peak, args.c3_n, args.c3_spokes)
-        if "c4" in want:
-            extra["c4"] = bench_c4(dev)
         if "c5" in want:
             extra["c5"] = bench_c5(dev)
 

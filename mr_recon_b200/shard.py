@@ -13,7 +13,7 @@ from typing import List, Sequence, Tuple
 
 import torch
 
-__all__ = ["shard_slices", "max_over_ranks"]
+__all__ = ["shard_slices", "max_over_ranks", "gather_slices"]
 
 
 def shard_slices(costs: Sequence[float], world: int, rank: int) -> Tuple[int, int]:
@@ -53,3 +53,25 @@ def max_over_ranks(value: float, device=None) -> float:
     t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def gather_slices(local: Sequence[torch.Tensor], begin: int, end: int, n_total: int) -> List[torch.Tensor]:
+    """The per-slice results of every rank, in slice order, on every rank.
+    ``local`` holds this rank's results for slices [begin, end) (tensors of
+    any shape, one per slice). Without a process group it returns ``local``.
+    The exchange is a host-side all_gather of objects: bookkeeping after a
+    solve, not part of the data path."""
+    import torch.distributed as dist
+    if len(local) != end - begin:
+        raise ValueError("one result per local slice is needed")
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return list(local)
+    parts = [None] * dist.get_world_size()
+    dist.all_gather_object(parts, (int(begin), [t.detach().cpu() for t in local]))
+    out: List = [None] * n_total
+    for b, ts in parts:
+        for i, t in enumerate(ts):
+            out[b + i] = t
+    if any(t is None for t in out):
+        raise RuntimeError("the ranks' slice ranges do not cover the batch")
+    return out
