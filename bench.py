@@ -55,9 +55,11 @@ TRAFFIC_SOURCE = ("ncu --set full capture of k_grid_reg<6,1> and k_interp_reg<2,
 CG_FIXTURE = os.path.join(ROOT, "tests", "golden", "cg_config2.npz")
 # Speed of the oracle port relative to the reference's own CPU path
 # (triton_nufft on CPU tensors, its torch fallback) on this workload: both
-# timed on the same 8 host threads of the development machine, 8 coils,
-# forward + adjoint (the reference cannot run where the benchmark runs).
-PORT_VS_REFERENCE = {"port_msample_coil_s": 0.40, "reference_msample_coil_s": 0.94, "threads": 8,
+# timed on the same 8 host threads of the development machine (Intel Xeon,
+# 2.7 GHz), 8 coils, forward + adjoint, median of 3 after a warm-up; their
+# forward outputs agree to 6e-7. The reference cannot run where the benchmark
+# runs, so the port stands in for it and is the slower of the two.
+PORT_VS_REFERENCE = {"port_msample_coil_s": 0.44, "reference_msample_coil_s": 1.03, "threads": 8,
                      "ratio": 0.43}
 
 
