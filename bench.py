@@ -473,12 +473,88 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_reference_gpu(args, rank):
+    """--impl reference_gpu (not part of the default runs): the reference's own
+    GPU NUFFT -- triton_nufft over its Triton interpolation and gridding
+    kernels (triton_interp/ungrid.py:154-846, grid.py:158-502) -- from the
+    unmodified package installed in baseline/_ref, on the headline workload
+    and on this GPU, timed with CUDA events after a warm-up that includes the
+    Triton compilation. Modules the KB path never calls (cupy, sigpy, ...) are
+    stubbed by tests/golden/refshim.py so the package imports."""
+    if rank != 0:
+        return
+    ref_dir = os.path.join(ROOT, "baseline", "_ref")
+    if not os.path.isdir(os.path.join(ref_dir, "mr_recon")):
+        print(json.dumps({"impl": "reference_gpu", "unavailable": "the reference is not installed in baseline/_ref"}))
+        return
+    os.environ.setdefault("TORCH_COMPILE_DISABLE", "1")
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import refshim
+    refshim.install(ref_dir)
+    import torch
+    from mr_recon.fourier import triton_nufft
+    dev = torch.device("cuda", 0)
+    _, _, imgs_np, trj_np = make_inputs(1234)
+    imgs = torch.from_numpy(imgs_np).to(dev)
+    trj = torch.from_numpy(trj_np).to(dev)
+    nf = triton_nufft(IM, oversamp=OS, width=W)
+    for _ in range(max(3, args.warmup)):
+        k = nf.forward(imgs, trj)
+        nf.adjoint(k, trj)
+    torch.cuda.synchronize()
+    e0, e1 = _events(torch)
+    e0.record()
+    for _ in range(args.steps):
+        k = nf.forward(imgs, trj)
+        b = nf.adjoint(k, trj)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    # the B200 path on the same inputs, for the relative difference of the results
+    from mr_recon_b200.fourier import b200_nufft
+    ours = b200_nufft(IM, oversamp=OS, width=W)
+    ko = ours.forward(imgs, trj)
+    bo = ours.adjoint(k, trj)
+    rel = lambda a, r: float((a - r).abs().square().sum().sqrt() / r.abs().square().sum().sqrt())  # noqa: E731
+    M = NINTL * NSAMP
+    # CG-SENSE with the reference's own linop and solver on its Triton NUFFT (all
+    # coils in one batch; max_eigen given, as the benchmark's CG-SENSE does)
+    from mr_recon.linops import batching_params, sense_linop
+    from mr_recon.recons import CG_SENSE_recon
+    from mr_recon_b200 import synth
+    x_np, mps_np, _, _ = make_inputs(1234)
+    A = sense_linop(trj[0], torch.from_numpy(mps_np).to(dev), nufft=nf,
+                    bparams=batching_params(coil_batch_size=NCOIL))
+    kk = A.forward(torch.from_numpy(x_np).to(dev))
+    kk = torch.from_numpy(synth.add_noise(kk.cpu().numpy(), 30.0, np.random.RandomState(99))).to(dev)
+    fix = np.load(CG_FIXTURE) if os.path.exists(CG_FIXTURE) else None
+    me = float(fix["max_eigen"]) if fix is not None else 1.0
+    xr = CG_SENSE_recon(A, kk, max_iter=20, lamda_l2=1e-3, max_eigen=me, verbose=False)
+    torch.cuda.synchronize()
+    e0.record()
+    reps = 3
+    for _ in range(reps):
+        xr = CG_SENSE_recon(A, kk, max_iter=20, lamda_l2=1e-3, max_eigen=me, verbose=False)
+    e1.record()
+    torch.cuda.synchronize()
+    cg_ms = e0.elapsed_time(e1) / reps
+    cg = {"solves_per_s": 1e3 / cg_ms, "ms_per_solve": cg_ms, "iterations": 20, "lambda": 1e-3,
+          "coil_batch_size": NCOIL}
+    if fix is not None:
+        ref = torch.from_numpy(fix["x_cg64"]).to(dev)
+        cg["rel_err_vs_oracle_cg64"] = rel(xr.reshape(ref.shape), ref)
+    print(json.dumps({"impl": "reference_gpu", "metric": METRIC, "value": NCOIL * M / (ms / 1e3) / 1e6,
+                      "unit": UNIT, "ms_per_step": ms, "steps": args.steps, "dtype": "complex64",
+                      "config": {"workload": WORKLOAD}, "cg_sense": cg,
+                      "rel_diff_vs_b200": {"forward": rel(ko, k), "adjoint": rel(bo, b)}}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference_gpu"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cg", action="store_true")
     ap.add_argument("--c3-n", type=int, default=192, help="c3 image edge (192 = the configuration)")
@@ -501,6 +577,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.impl == "reference_gpu":
+        run_reference_gpu(args, rank)
         return
 
     import torch
