@@ -23,29 +23,87 @@ namespace mrn {
 // and group of at most 16 coils; the tile is at most 8x8x8 cells. Thread =
 // (coil = lane & 15, x-plane p = 2 warp + lane / 16); it keeps all 8 (y) x 8
 // (z) complex cells of its plane in registers, so every update is a register
-// FMA with a compile-time index. Per entry each thread reads the tile-aligned
-// weight of its plane (zero outside the footprint) and the tile-aligned y and
-// z weights; y-rows without weight are skipped by a warp-uniform branch and
-// each remaining row takes 8 packed two-lane FMAs along z (fma.rn.f32x2: re
-// and im of one cell). There is no data-dependent dispatch: control flow is
-// uniform in the warp, and each warp takes one ballot per 32 entries of those
-// with weight on its two planes.
+// FMA with a compile-time index.
 //
-// The tile-aligned weights (x carrying the scale) and the sample values
-// reach shared memory in batches of 64 entries through a cp.async pipeline:
-// in iteration b the values of batch b+1 and the coordinates of batch b+3
-// are in flight while the weights of batch b+1 are evaluated (the K candidate
-// taps of each dimension, written to their cells) and batch b is accumulated;
-// one barrier per batch. No atomics; float32 accumulation in entry order, so
-// results are the same on every run (split tiles write partial tiles that a
-// reduction pass adds in item order).
+// Footprint windows. With K candidate taps per dimension a sample's footprint
+// has K - 1 = KW taps per dimension unless u - W/2 is an integer (then the
+// K-th candidate lies exactly on the support boundary and carries weight), so
+// in y and z the part of a footprint inside the tile fits a window of KW
+// cells starting at w0 in [0, NW), NW = 8 - KW + 1 (clamped to the tile; a
+// footprint that is cut by the tile edge has zero weights in the window's
+// outside cells). The window start pair (y0, z0) is the same for every
+// thread of the CTA (they all accumulate the same entry), so one warp-uniform
+// binary dispatch over the NW^2 pairs selects a straight-line block of KW
+// rows x KW cells of packed two-lane FMAs (fma.rn.f32x2: re and im of a
+// cell) on fixed registers: no FMA touches a cell outside the window and no
+// row needs a test. Entries with K taps inside the tile in y or z (exact
+// boundary taps) take the dense block: tile-aligned weights, warp-uniform
+// skips of rows without weight, 8 cells per row.
+//
+// The weights (x tile-aligned and carrying the scale; y and z both as windows
+// and tile-aligned) and the sample values reach shared memory in batches of
+// 64 entries through a cp.async pipeline: in iteration b the values of batch
+// b+1 and the coordinates of batch b+3 are in flight while the weights of
+// batch b+1 are evaluated and batch b is accumulated; one barrier per batch.
+// Each warp takes one ballot per 32 entries of those with weight on its two
+// planes. No atomics; float32 accumulation in entry order, so results are the
+// same on every run (split tiles write partial tiles that a reduction pass
+// adds in item order).
 // ---------------------------------------------------------------------------
 constexpr int kG3Tile = 8;
 constexpr int kG3Batch = 64;
 constexpr int kG3Coils = 16;
 constexpr int kG3Threads = 128;
 
-template <int K>
+namespace {
+
+template <int B>
+struct G3Smem {
+  float4 c[3][B];        // coordinate ring
+  int pm[3][B];          // sample index ring
+  float wx[2][B][8];     // per entry: tile-aligned x weights x scale
+  float wyt[2][B][8];    // per entry: tile-aligned y weights (dense block)
+  float wzt[2][B][8];    // per entry: tile-aligned z weights (dense block)
+  float wyw[2][B][8];    // per entry: y weights of the window (first KW used)
+  float2 wzw[2][B][8];   // per entry: z weights of the window, each twice
+  int2 code[2][B];       // per entry: window starts (y0, z0); NW = dense
+  float2 v[2][B][kG3Coils];  // per entry and coil: sample value
+  float d[2][B];         // per entry: density weight
+  float2 t[2][B];        // per entry: temporal weight
+};
+
+// KW rows x KW cells of the window at (Y0, Z0): acc[Y0 + r][Z0 + c] +=
+// wy[r] wz[c] v for the thread's coil and plane (v already carries the x
+// weight and the scale).
+template <int KW, int Y0, int Z0>
+__device__ __forceinline__ void win_block(float2 (&acc)[kG3Tile][kG3Tile], const float (&wy)[KW],
+                                          const float2 (&wz)[KW], float2 v) {
+#pragma unroll
+  for (int r = 0; r < KW; ++r) {
+    const float2 v2 = __fmul2_rn(make_float2(wy[r], wy[r]), v);
+#pragma unroll
+    for (int c = 0; c < KW; ++c) acc[Y0 + r][Z0 + c] = __ffma2_rn(wz[c], v2, acc[Y0 + r][Z0 + c]);
+  }
+}
+
+// Binary dispatch of the window code y0 * NW + z0 over [LO, HI).
+template <int KW, int NW, int LO, int HI>
+struct WinDispatch {
+  static __device__ __forceinline__ void run(int code, float2 (&acc)[kG3Tile][kG3Tile],
+                                             const float (&wy)[KW], const float2 (&wz)[KW], float2 v) {
+    if constexpr (HI - LO == 1) {
+      win_block<KW, LO / NW, LO % NW>(acc, wy, wz, v);
+    } else {
+      constexpr int MID = (LO + HI) / 2;
+      if (code < MID) WinDispatch<KW, NW, LO, MID>::run(code, acc, wy, wz, v);
+      else WinDispatch<KW, NW, MID, HI>::run(code, acc, wy, wz, v);
+    }
+  }
+};
+
+}  // namespace
+
+template <int K, bool EXTRA>
 __global__ void __launch_bounds__(kG3Threads, 3)
 k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBParams kb,
             const float4* __restrict__ coord, const int* __restrict__ perm,
@@ -53,16 +111,11 @@ k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
             const float2* __restrict__ temporal, float2* __restrict__ grid, int layout, float scale,
             int cg, SplitOut so) {
   constexpr int T = kG3Tile, B = kG3Batch, CW = kG3Coils, NT = kG3Threads;
+  constexpr int KW = K - 1, NW = T - KW + 1;
   static_assert(K <= T, "taps per dimension");
   static_assert(NT == 2 * B, "copy roles assume two threads per batch entry");
-  __shared__ float4 s_c[3][B];        // coordinate ring
-  __shared__ int s_pm[3][B];          // sample index ring
-  __shared__ float s_wx[2][B][T];     // per entry: tile-aligned x weights x scale
-  __shared__ float4 s_wy[2][B][2];    // per entry: tile-aligned y weights
-  __shared__ float4 s_wz[2][B][4];    // per entry: tile-aligned z weights, each twice
-  __shared__ float2 s_v[2][B][CW];    // per entry and coil: sample value
-  __shared__ float s_d[2][B];         // per entry: density weight
-  __shared__ float2 s_t[2][B];        // per entry: temporal weight
+  extern __shared__ __align__(16) unsigned char g3_smem[];
+  G3Smem<B>& s = *reinterpret_cast<G3Smem<B>*>(g3_smem);
 
   const Item it = items[blockIdx.x];
   if (it.slice < 0) return;  // padding past the real items
@@ -83,57 +136,86 @@ k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
   // coordinates and sample indices of batch bi into ring slot bi % 3
   auto copy_coords = [&](int bi) {
     const int nb = batch_len(bi), r3 = bi % 3;
-    if (tid < nb) cp_async16(&s_c[r3][tid], coord + it.start + bi * B + tid);
-    else if (tid >= B && tid - B < nb) cp_async4(&s_pm[r3][tid - B], perm + it.start + bi * B + tid - B);
+    if (tid < nb) cp_async16(&s.c[r3][tid], coord + it.start + bi * B + tid);
+    else if (tid >= B && tid - B < nb) cp_async4(&s.pm[r3][tid - B], perm + it.start + bi * B + tid - B);
   };
   // sample values (one 8-byte copy per entry and coil), densities, temporal weights
   auto copy_values = [&](int bi) {
     const int nb = batch_len(bi), b2 = bi & 1, r3 = bi % 3;
     for (int k = tid; k < B * CW; k += NT) {
       const int j = k >> 4, c = k & 15;
-      if (j < nb && c < ncg) cp_async8(&s_v[b2][j][c], kspg + (int64_t)c * m + (s_pm[r3][j] - pt_off));
+      if (j < nb && c < ncg) cp_async8(&s.v[b2][j][c], kspg + (int64_t)c * m + (s.pm[r3][j] - pt_off));
     }
-    if (tid < nb) {
-      if (dcf) cp_async4(&s_d[b2][tid], dcf + s_pm[r3][tid]);
-    } else if (tid >= B && tid - B < nb) {
-      if (temporal) cp_async8(&s_t[b2][tid - B], temporal + s_pm[r3][tid - B]);
+    if (EXTRA) {
+      if (tid < nb) {
+        if (dcf) cp_async4(&s.d[b2][tid], dcf + s.pm[r3][tid]);
+      } else if (tid >= B && tid - B < nb) {
+        if (temporal) cp_async8(&s.t[b2][tid - B], temporal + s.pm[r3][tid - B]);
+      }
     }
   };
-  // unit (entry j, dimension i): the K candidate taps' weights, written to
-  // their cells of the tile-aligned weight vector (zero elsewhere)
+  // unit (entry j, dimension i): the K candidate taps' weights; x as a
+  // tile-aligned vector, y and z as tile-aligned vectors and as windows
   auto weights = [&](int bi) {
     const int nb = batch_len(bi), b2 = bi & 1, r3 = bi % 3;
-    for (int t = tid; t < 3 * B; t += NT) {
+    // 3B units over NT threads; later rounds start at the other half of the
+    // CTA, so the threads with a unit more are spread over the warps
+    for (int rnd = 0; rnd * NT < 3 * B; ++rnd) {
+      const int t = rnd * NT + (tid + rnd * (NT / 2)) % NT;
+      if (t >= 3 * B) continue;
       const int j = t / 3, i = t - 3 * j;
       if (j >= nb) continue;
-      const float4 c4 = s_c[r3][j];
+      const float4 c4 = s.c[r3][j];
       const float u = i == 0 ? c4.x : (i == 1 ? c4.y : c4.z);
       const float r = sel3(kb.radius, i), ir = sel3(kb.inv_radius, i);
       const int n = sel3(gp->nos, i), size = sel3(f.size, i);
       const int lo = (int)ceilf(__fsub_rn(u, r));
       int st = wrap_once(lo, n) - sel3(f.org, i);
       if (st >= size) st -= n;  // footprint wraps into this tile from the end
-      float w[T];
-#pragma unroll
-      for (int cell = 0; cell < T; ++cell) w[cell] = 0.f;
+      float wq[K];
+      bool last = false;  // the K-th candidate tap carries weight
 #pragma unroll
       for (int q = 0; q < K; ++q) {
         const int cell = st + q;
         const float adx = fabsf(__fsub_rn((float)(lo + q), u));
-        const float wq = (cell >= 0 && cell < size && adx <= r) ? kb_tap_fast(adx, ir, kb) : 0.f;
+        if (q == K - 1) last = adx <= r;
+        wq[q] = (cell >= 0 && cell < size && adx <= r) ? kb_tap_fast(adx, ir, kb) : 0.f;
+      }
+      float w[T];
 #pragma unroll
-        for (int c = 0; c < T; ++c)
-          if (c == cell) w[c] = wq;
+      for (int c = 0; c < T; ++c) {
+        w[c] = 0.f;
+#pragma unroll
+        for (int q = 0; q < K; ++q)
+          if (st + q == c) w[c] = wq[q];
       }
       if (i == 0) {
 #pragma unroll
-        for (int c = 0; c < T; ++c) s_wx[b2][j][c] = w[c] * scale;
-      } else if (i == 1) {
-        s_wy[b2][j][0] = make_float4(w[0], w[1], w[2], w[3]);
-        s_wy[b2][j][1] = make_float4(w[4], w[5], w[6], w[7]);
+        for (int c = 0; c < T; ++c) s.wx[b2][j][c] = w[c] * scale;
+        continue;
+      }
+      float* wt = i == 1 ? s.wyt[b2][j] : s.wzt[b2][j];
+      *reinterpret_cast<float4*>(wt) = make_float4(w[0], w[1], w[2], w[3]);
+      *reinterpret_cast<float4*>(wt + 4) = make_float4(w[4], w[5], w[6], w[7]);
+      // window of KW cells from w0; K taps inside the tile do not fit one
+      const bool dense = last && st >= 0 && st + K <= size;
+      const int w0 = dense ? NW : min(max(st, 0), size - KW);
+      float ww[KW];
+#pragma unroll
+      for (int c = 0; c < KW; ++c) {
+        ww[c] = 0.f;
+#pragma unroll
+        for (int q = 0; q < K; ++q)
+          if (st + q == w0 + c) ww[c] = wq[q];
+      }
+      if (i == 1) {
+#pragma unroll
+        for (int c = 0; c < KW; ++c) s.wyw[b2][j][c] = ww[c];
+        s.code[b2][j].x = w0;
       } else {
 #pragma unroll
-        for (int c = 0; c < T / 2; ++c) s_wz[b2][j][c] = make_float4(w[2 * c], w[2 * c], w[2 * c + 1], w[2 * c + 1]);
+        for (int c = 0; c < KW; ++c) s.wzw[b2][j][c] = make_float2(ww[c], ww[c]);
+        s.code[b2][j].y = w0;
       }
     }
   };
@@ -167,66 +249,99 @@ k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
     for (int h32 = 0; h32 < B; h32 += 32) {
       bool meet = false;
       if (h32 + lane < nb) {
-        const float2 xw = *reinterpret_cast<const float2*>(&s_wx[b2][h32 + lane][2 * warp]);
+        const float2 xw = *reinterpret_cast<const float2*>(&s.wx[b2][h32 + lane][2 * warp]);
         meet = xw.x != 0.f || xw.y != 0.f;
       }
       unsigned act = __ballot_sync(0xffffffffu, meet);
       while (act) {
         const int j = h32 + __ffs(act) - 1;
         act &= act - 1u;
-        const float wx = s_wx[b2][j][plane];
-        float2 val = has_coil ? s_v[b2][j][coil] : make_float2(0.f, 0.f);
-        if (dcf) {
-          const float d = s_d[b2][j];
-          val = make_float2(val.x * d, val.y * d);
-        }
-        if (temporal) {  // times conj(t)
-          const float2 tt = s_t[b2][j];
-          val = make_float2(val.x * tt.x + val.y * tt.y, val.y * tt.x - val.x * tt.y);
+        const float wx = s.wx[b2][j][plane];
+        float2 val = has_coil ? s.v[b2][j][coil] : make_float2(0.f, 0.f);
+        if (EXTRA) {
+          if (dcf) {
+            const float d = s.d[b2][j];
+            val = make_float2(val.x * d, val.y * d);
+          }
+          if (temporal) {  // times conj(t)
+            const float2 tt = s.t[b2][j];
+            val = make_float2(val.x * tt.x + val.y * tt.y, val.y * tt.x - val.x * tt.y);
+          }
         }
         const float2 v = __fmul2_rn(make_float2(wx, wx), val);
-        const float4 y0 = s_wy[b2][j][0], y1 = s_wy[b2][j][1];
-        const float wy[T] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
-        float2 wz[T];
+        const int2 code = s.code[b2][j];
+        if (code.x < NW && code.y < NW) {  // uniform: the whole CTA shares the entry
+          float wy[KW];
+          float2 wz[KW];
 #pragma unroll
-        for (int c = 0; c < T / 2; ++c) {
-          const float4 z4 = s_wz[b2][j][c];
-          wz[2 * c] = make_float2(z4.x, z4.y);
-          wz[2 * c + 1] = make_float2(z4.z, z4.w);
-        }
+          for (int c = 0; c < KW; ++c) {
+            wy[c] = s.wyw[b2][j][c];
+            wz[c] = s.wzw[b2][j][c];
+          }
+          WinDispatch<KW, NW, 0, NW * NW>::run(code.x * NW + code.y, acc, wy, wz, v);
+        } else {
+          float wy[T];
+          float2 wz[T];
 #pragma unroll
-        for (int y = 0; y < T; ++y) {
-          if (wy[y] == 0.f) continue;  // uniform: the whole warp shares the entry
-          const float2 v2 = __fmul2_rn(make_float2(wy[y], wy[y]), v);
+          for (int c = 0; c < T; ++c) {
+            wy[c] = s.wyt[b2][j][c];
+            const float z = s.wzt[b2][j][c];
+            wz[c] = make_float2(z, z);
+          }
 #pragma unroll
-          for (int z = 0; z < T; ++z) acc[y][z] = __ffma2_rn(wz[z], v2, acc[y][z]);
+          for (int y = 0; y < T; ++y) {
+            if (wy[y] == 0.f) continue;  // uniform
+            const float2 v2 = __fmul2_rn(make_float2(wy[y], wy[y]), v);
+#pragma unroll
+            for (int z = 0; z < T; ++z) acc[y][z] = __ffma2_rn(wz[z], v2, acc[y][z]);
+          }
         }
       }
     }
   }
   cp_async_wait<0>();
 
-  if (has_coil && plane < f.size[0]) {
-    const int nos0 = gp->nos[0], nos1 = gp->nos[1], nos2 = gp->nos[2];
-    const int hs0 = layout == kInternal ? gp->hshift[0] : 0;
-    const int hs1 = layout == kInternal ? gp->hshift[1] : 0;
-    const int hs2 = layout == kInternal ? gp->hshift[2] : 0;
-    float2* dst = grid + (layout == kInternal ? gp->grid_off : gp->ugrid_off) + (int64_t)(c0 + coil) * gp->gos;
-    const int64_t xo = (int64_t)wrap_once(f.org[0] + plane - hs0, nos0) * nos1;
-    const int zs = wrap_once(f.org[2] - hs2, nos2);
+  // Write-back through shared memory, half the tile (four x-planes) at a
+  // time: the two warps holding those planes store their cells as 64 blocks
+  // (plane, coil) of 8x8 cells (block stride 65 cells: conflict-free 8-byte
+  // stores), then all threads store them out with consecutive lanes on
+  // consecutive z-cells of a row, so one warp store covers four 64-byte rows
+  // instead of 32 scattered 8-byte cells.
+  constexpr int CS = T * T + 1;
+  static_assert(64 * CS * sizeof(float2) <= sizeof(G3Smem<B>), "write-back staging fits");
+  float2* stage = reinterpret_cast<float2*>(g3_smem);
+  const int nos0 = gp->nos[0], nos1 = gp->nos[1], nos2 = gp->nos[2];
+  const int hs0 = layout == kInternal ? gp->hshift[0] : 0;
+  const int hs1 = layout == kInternal ? gp->hshift[1] : 0;
+  const int hs2 = layout == kInternal ? gp->hshift[2] : 0;
+  float2* dst = grid + (layout == kInternal ? gp->grid_off : gp->ugrid_off) + (int64_t)c0 * gp->gos;
+  // this thread's cell of every block it stores: (y, z) fixed, block varies
+  const int cell = tid & 63, cy = cell >> 3, cz = cell & 7;
+  const bool cell_in = cy < f.size[1] && cz < f.size[2];
+  int zz = wrap_once(f.org[2] - hs2, nos2) + cz;
+  if (zz >= nos2) zz -= nos2;
+  const int64_t yz = (int64_t)wrap_once(f.org[1] + cy - hs1, nos1) * nos2 + zz;
+#pragma unroll 1
+  for (int half = 0; half < 2; ++half) {
+    __syncthreads();  // staging buffers free (batch buffers, or the previous half)
+    if ((warp >> 1) == half) {
+      float2* b = stage + ((warp & 1) * 32 + lane) * CS;  // block = (plane - 4 half) * 16 + coil
 #pragma unroll
-    for (int y = 0; y < T; ++y) {
-      if (y >= f.size[1]) break;
-      float2* rowp = dst + (xo + wrap_once(f.org[1] + y - hs1, nos1)) * nos2;
+      for (int y = 0; y < T; ++y)
 #pragma unroll
-      for (int z = 0; z < T; ++z) {
-        if (z >= f.size[2]) break;
-        int zz = zs + z;
-        if (zz >= nos2) zz -= nos2;
-        if (it.split)
-          *split_slot(so, it.split, c0 + coil, (plane * f.size[1] + y) * f.size[2] + z) = acc[y][z];
-        else
-          rowp[zz] = acc[y][z];
+        for (int z = 0; z < T; ++z) b[y * T + z] = acc[y][z];
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int blk = tid >> 6; blk < 64; blk += NT / 64) {
+      const int bc = blk & 15, bp = 4 * half + (blk >> 4);
+      if (!cell_in || bc >= ncg || bp >= f.size[0]) continue;
+      const float2 val = stage[blk * CS + cell];
+      if (it.split) {
+        *split_slot(so, it.split, c0 + bc, (bp * f.size[1] + cy) * f.size[2] + cz) = val;
+      } else {
+        const int64_t xo = (int64_t)wrap_once(f.org[0] + bp - hs0, nos0) * nos1 * nos2;
+        dst[(int64_t)bc * gp->gos + xo + yz] = val;
       }
     }
   }
@@ -247,14 +362,24 @@ int launch_grid_reg3(mrn_plan* P, const float2* ksp, const float* dcf, const flo
   const dim3 gdim((unsigned)P->n_items_grid, (unsigned)ng);
   const int K = P->kb.ntaps[0];
   const SplitOut so = split_out(P);
-#define MRN_G3_LAUNCH(KK)                                                                         \
-  k_grid_reg3<KK><<<gdim, kG3Threads, 0, st>>>(P->d_items_g, P->d_slices, P->kb, P->d_coord_g,    \
-                                               P->d_perm_g, ksp, dcf, temporal, grid, layout, scale, cg, so)
-  if (K == 5) MRN_G3_LAUNCH(5);
-  else if (K == 6) MRN_G3_LAUNCH(6);
-  else if (K == 7) MRN_G3_LAUNCH(7);
-  else MRN_G3_LAUNCH(8);
+  const size_t smem = sizeof(G3Smem<kG3Batch>);
+  const bool extra = dcf != nullptr || temporal != nullptr;
+  int rc = MRN_OK;
+#define MRN_G3_LAUNCH(KK, EX)                                                                     \
+  do {                                                                                            \
+    auto kern = k_grid_reg3<KK, EX>;                                                              \
+    rc = set_dynamic_smem(kern, smem);                                                            \
+    if (rc == MRN_OK)                                                                             \
+      kern<<<gdim, kG3Threads, smem, st>>>(P->d_items_g, P->d_slices, P->kb, P->d_coord_g,        \
+                                           P->d_perm_g, ksp, dcf, temporal, grid, layout, scale, \
+                                           cg, so);                                               \
+  } while (0)
+  if (K == 5) { if (extra) MRN_G3_LAUNCH(5, true); else MRN_G3_LAUNCH(5, false); }
+  else if (K == 6) { if (extra) MRN_G3_LAUNCH(6, true); else MRN_G3_LAUNCH(6, false); }
+  else if (K == 7) { if (extra) MRN_G3_LAUNCH(7, true); else MRN_G3_LAUNCH(7, false); }
+  else { if (extra) MRN_G3_LAUNCH(8, true); else MRN_G3_LAUNCH(8, false); }
 #undef MRN_G3_LAUNCH
+  if (rc != MRN_OK) return rc;
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? MRN_OK : cuda_fail(e);
 }

@@ -87,6 +87,23 @@ def test_noalloc_interp_matches_plan_interp_on_two_calls():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("grid_size,width,beta,ncoil,npts", [
+    ((300,), (6.0,), 10.95, 4, 3000),                # 1D
+    ((64, 72), (5.5, 3.0), 9.0, 3, 8000),            # 2D, non-integer and unequal widths
+    ((18, 20, 16), (4.0, 6.0, 5.0), 8.0, 2, 5000),   # 3D, a different width per axis
+])
+def test_noalloc_interp_per_axis_widths(grid_size, width, beta, ncoil, npts):
+    # the per-axis tap count differs from the largest one (the scratch stride)
+    # here, which is the layout-sensitive part of the weight and gather kernels
+    rng = np.random.RandomState(sum(grid_size))
+    g, locs = _case(rng, grid_size, ncoil, npts)
+    for _ in range(2):
+        out = _noalloc_interp(grid_size, width, beta, g, locs)
+        ref = _regular_interp(grid_size, width, beta, g, locs)
+        assert _rel(out, ref) < TOL
+
+
+@pytest.mark.gpu
 def test_noalloc_interp_rejects_oversized_problem():
     lib = _lib.load()
     # 4M samples of 2D width 6 need 256 MiB of scratch: refused before any launch
