@@ -915,6 +915,23 @@ k_trajgrad_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl,
 constexpr int kRegTile = 8;
 constexpr int kRegRows = kRegTile / 2;  // tile rows per warp
 constexpr int kRegBatch = 16;
+constexpr int kRegStage = kRegTile * kRegTile + 1;  // cells per coil block in the write-back, padded
+
+// Shared memory of k_grid_reg: the batch pipeline's buffers, reused after the
+// last batch to stage the tile for the write-back.
+template <int CW>
+union G2Smem {
+  struct {
+    float4 c[3][kRegBatch];      // coordinate ring
+    int pm[3][kRegBatch];        // sample index ring
+    float4 wr[2][kRegBatch][2];  // per entry: row weights x scale (cells 0-7)
+    float4 wc[2][kRegBatch][4];  // per entry: column weights, each twice (cells 0-7)
+    float2 v[2][kRegBatch][CW];  // per entry and coil: sample value
+    float d[2][kRegBatch];       // per entry: density weight
+    float2 t[2][kRegBatch];      // per entry: temporal weight
+  } b;
+  float2 stage[CW][kRegStage];   // write-back: per coil, the tile's cells row-major
+};
 
 template <int K, int SUB>
 __global__ void __launch_bounds__(64, 8)
@@ -924,13 +941,14 @@ k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBP
            const float2* __restrict__ temporal, float2* __restrict__ grid, int layout, float scale,
            int cg, SplitOut so) {
   constexpr int T = kRegTile, R = kRegRows, B = kRegBatch, CW = 32 / SUB;
-  __shared__ float4 s_c[3][B];      // coordinate ring
-  __shared__ int s_pm[3][B];        // sample index ring
-  __shared__ float4 s_wr[2][B][2];  // per entry: row weights x scale (cells 0-7)
-  __shared__ float4 s_wc[2][B][4];  // per entry: column weights, each twice (cells 0-7)
-  __shared__ float2 s_v[2][B][CW];  // per entry and coil: sample value
-  __shared__ float s_d[2][B];       // per entry: density weight
-  __shared__ float2 s_t[2][B];      // per entry: temporal weight
+  __shared__ G2Smem<CW> sm;
+  auto& s_c = sm.b.c;
+  auto& s_pm = sm.b.pm;
+  auto& s_wr = sm.b.wr;
+  auto& s_wc = sm.b.wc;
+  auto& s_v = sm.b.v;
+  auto& s_d = sm.b.d;
+  auto& s_t = sm.b.t;
 
   const Item it = items[blockIdx.x];
   if (it.slice < 0) return;  // padding past the real items
@@ -1062,25 +1080,31 @@ k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBP
           acc[a][b].y += __shfl_xor_sync(0xffffffffu, acc[a][b].y, o);
         }
   }
+  // Write-back through shared memory: each lane stores its coil's cells as a
+  // row-major block (stride 65 cells: conflict-free 8-byte stores), then
+  // thread t stores cell t of every coil block, so one warp store covers four
+  // 64-byte rows of one coil instead of 32 coils' scattered 8-byte cells.
+  __syncthreads();  // batch buffers no longer read
   if (has_coil && sub == 0) {
+#pragma unroll
+    for (int a = 0; a < R; ++a)
+#pragma unroll
+      for (int b = 0; b < T; ++b) sm.stage[coil][(warp * R + a) * T + b] = acc[a][b];
+  }
+  __syncthreads();
+  const int row = tid >> 3, col = tid & 7;
+  if (row < f.size[0] && col < f.size[1]) {
     const int hs0 = layout == kInternal ? gp->hshift[0] : 0;
     const int hs1 = layout == kInternal ? gp->hshift[1] : 0;
     const int64_t gos = gp->gos;
-    float2* dst = grid + (layout == kInternal ? gp->grid_off : gp->ugrid_off) + (int64_t)(c0 + coil) * gos;
-    const int s1 = wrap_once(f.org[1] - hs1, nos1);
-#pragma unroll
-    for (int a = 0; a < R; ++a) {
-      const int row = warp * R + a;
-      if (row >= f.size[0]) break;
-      const int64_t rowo = (int64_t)wrap_once(f.org[0] + row - hs0, nos0) * nos1;
-#pragma unroll
-      for (int b = 0; b < T; ++b) {
-        if (b >= f.size[1]) break;
-        int s = s1 + b;
-        if (s >= nos1) s -= nos1;
-        if (it.split) *split_slot(so, it.split, c0 + coil, row * f.size[1] + b) = acc[a][b];
-        else dst[rowo + s] = acc[a][b];
-      }
+    float2* dst = grid + (layout == kInternal ? gp->grid_off : gp->ugrid_off) + (int64_t)c0 * gos +
+                  (int64_t)wrap_once(f.org[0] + row - hs0, nos0) * nos1 + wrap_once(f.org[1] + col - hs1, nos1);
+    const int scell = row * f.size[1] + col;
+#pragma unroll 4
+    for (int c = 0; c < ncg; ++c) {
+      const float2 val = sm.stage[c][tid];
+      if (it.split) *split_slot(so, it.split, c0 + c, scell) = val;
+      else dst[(int64_t)c * gos] = val;
     }
   }
 }
