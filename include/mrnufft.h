@@ -203,6 +203,32 @@ int mrn_sense_normal(mrn_plan* plan, const void* x, const void* mps, const float
                      void* stream);
 
 /*
+ * Low-rank SENSE operators: time-segmented off-resonance models with any
+ * temporal interpolators (sense_linop with spatial_funcs / temporal_funcs,
+ * linops.py:1134-1228, e.g. alpha_segementation's least-squares h_l(t),
+ * imperfections/field.py:272-369) and subspace models (subspace_linop,
+ * linops.py:1496-1772; subspace_linop_new, 1379-1495). The plan's slices are
+ * the J components (a segment, or a subspace coefficient and segment): all
+ * slices have the same image size, coil count C and sample count M, and the
+ * same trajectory (bound once per slice, back to back). x / out hold one
+ * component image per slice (b_l times the coefficient volume, the caller's
+ * elementwise product), mps per slice [C][N...], w per slice [M] complex64
+ * (the component's temporal weight h_l(t) phi_k(t)); ksp is one [C][M] block.
+ *   mrn_lr_forward: ksp[c][t] = sum_j w[j][t] NUFFT_j(mps[j][c] x[j])[t]
+ *                   (components summed in order)
+ *   mrn_lr_adjoint: x[j] = out_scale sum_c conj(mps[j][c]) NUFFT_j^H(conj(w[j]) ksp[c])
+ *                   (fold a density compensation into w: it is real)
+ *   mrn_lr_normal : out[j] = out_scale lr_adjoint(lr_forward(x; w_fwd); w_adj)[j] + lam x[j]
+ * MRN_ERR_ARG when the slices differ in coil or sample count.
+ */
+int mrn_lr_forward(mrn_plan* plan, const void* x, const void* mps, const void* w, void* ksp,
+                   void* stream);
+int mrn_lr_adjoint(mrn_plan* plan, const void* ksp, const void* w, const void* mps, void* x,
+                   float out_scale, void* stream);
+int mrn_lr_normal(mrn_plan* plan, const void* x, const void* mps, const void* w_fwd, const void* w_adj,
+                  void* out, float out_scale, float lam, void* stream);
+
+/*
  * Toeplitz (FFT-only) normal operator A^H A, for plans without MRN_PLAN_RAW.
  * Replaces NUFFT.normal_toeplitz (fourier.py:302-352) and the Toeplitz branch
  * of sense_linop.normal (linops.py:1249-1308) for one image per slice and no

@@ -13,7 +13,7 @@ __version__ = "0.1.0"
 
 from . import _lib  # noqa: F401
 from .fourier import NUFFT, b200_nufft, triton_nufft, calc_toep_kernel_helper  # noqa: F401
-from .linops import batching_params, linop, sense_linop  # noqa: F401
+from .linops import batching_params, linop, sense_linop, subspace_linop, subspace_linop_new  # noqa: F401
 from .algs import conjugate_gradient, power_method_operator, FISTA, gradient_descent, SenseCG  # noqa: F401
 from .recons import CG_SENSE_recon, FISTA_recon, min_norm_recon, coil_combine  # noqa: F401
 from .plan import Plan  # noqa: F401

@@ -71,6 +71,9 @@ SIGNATURES = {
     "mrn_sense_forward": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "mrn_sense_adjoint": (_i, [_vp, _vp, _vp, _vp, _vp, _f, _vp]),
     "mrn_sense_normal": (_i, [_vp, _vp, _vp, _vp, _vp, _f, _f, _vp, _i, _vp]),
+    "mrn_lr_forward": (_i, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "mrn_lr_adjoint": (_i, [_vp, _vp, _vp, _vp, _vp, _f, _vp]),
+    "mrn_lr_normal": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _f, _f, _vp]),
     "mrn_plan_set_toeplitz": (_i, [_vp, _pi, _vp, _vp]),
     "mrn_toeplitz_normal": (_i, [_vp, _vp, _vp, _vp]),
     "mrn_sense_normal_toeplitz": (_i, [_vp, _vp, _vp, _vp, _f, _f, _vp, _i, _vp]),

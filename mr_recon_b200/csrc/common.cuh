@@ -321,6 +321,9 @@ struct mrn_plan {
 
   // device buffers
   mrn::SliceGeom* d_slices = nullptr;
+  // the slice table with every k-space offset 0: gridding through it reads
+  // one shared [C][M] k-space block for all slices (low-rank adjoint, lowrank.cu)
+  mrn::SliceGeom* d_slices_kshared = nullptr;
   float* d_apod = nullptr;          // apodization tables
   float4* d_coord_i = nullptr;      // interp-sorted scaled coords
   int* d_perm_i = nullptr;          // interp-sorted global point ids

@@ -343,6 +343,16 @@ StageTimer::~StageTimer() {
   if (idx >= 0) cudaEventRecord(P->timing_recs[idx].b, st);
 }
 
+// Upload the slice table and its shared-k-space twin (every ksp_off 0).
+static cudaError_t upload_slices(mrn_plan* P) {
+  cudaError_t e = cudaMemcpy(P->d_slices, P->h_slices.data(), P->nslices * sizeof(SliceGeom),
+                             cudaMemcpyHostToDevice);
+  if (e != cudaSuccess || !P->d_slices_kshared) return e;
+  std::vector<SliceGeom> ks(P->h_slices);
+  for (auto& g : ks) g.ksp_off = 0;
+  return cudaMemcpy(P->d_slices_kshared, ks.data(), P->nslices * sizeof(SliceGeom), cudaMemcpyHostToDevice);
+}
+
 template <class T>
 static int dev_alloc(T** p, size_t n) {
   if (*p) { cudaFree(*p); *p = nullptr; }
@@ -376,8 +386,7 @@ static int retile(mrn_plan* P) {
     P->cap_tiles = need;
   }
   cudaError_t e = cudaSetDevice(P->device);
-  if (e == cudaSuccess)
-    e = cudaMemcpy(P->d_slices, P->h_slices.data(), P->nslices * sizeof(SliceGeom), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = upload_slices(P);
   return e == cudaSuccess ? MRN_OK : cuda_fail(e);
 }
 
@@ -610,7 +619,8 @@ int mrn_plan_create(mrn_plan** out, int ndim, int n_slices, const int* im_size,
   int rc = MRN_OK;
 #define PK(x) do { rc = (x); if (rc != MRN_OK) { mrn_plan_destroy(P); return rc; } } while (0)
   PK(dev_alloc(&P->d_slices, n_slices));
-  e = cudaMemcpy(P->d_slices, P->h_slices.data(), n_slices * sizeof(SliceGeom), cudaMemcpyHostToDevice);
+  PK(dev_alloc(&P->d_slices_kshared, n_slices));
+  e = upload_slices(P);
   if (e != cudaSuccess) { mrn_plan_destroy(P); return cuda_fail(e); }
 
   // Apodization tables a(x) = sqrt(beta^2 - (pi W x)^2) / sinh(.), x = (q - N//2)/Nos
@@ -742,7 +752,7 @@ int mrn_plan_destroy(mrn_plan* P) {
   for (auto& fg : P->fft)
     if (fg.handle) cufftDestroy(fg.handle);
   toep_free(P);
-  void* bufs[] = {P->d_slices, P->d_apod, P->d_coord_i, P->d_perm_i, P->d_coord_g, P->d_perm_g,
+  void* bufs[] = {P->d_slices, P->d_slices_kshared, P->d_apod, P->d_coord_i, P->d_perm_i, P->d_coord_g, P->d_perm_g,
                   P->d_key_a, P->d_key_b, P->d_key_is, P->d_key_g, P->d_val_a, P->d_val_b, P->d_coord_tmp,
                   P->d_entry_cnt, P->d_tile_start_i, P->d_tile_end_i, P->d_tile_start_g,
                   P->d_tile_end_g, P->d_tile_nitems, P->d_tile_item_off, P->d_items_i,

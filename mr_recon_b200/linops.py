@@ -27,7 +27,8 @@ from .utils import PadLast, batch_iterator, fft, ifft, resize
 complex_dtype = torch.complex64
 real_dtype = torch.float32
 
-__all__ = ["batching_params", "linop", "sense_linop", "type3_nufft", "type3_nufft_naive"]
+__all__ = ["batching_params", "linop", "sense_linop", "subspace_linop", "subspace_linop_new", "type3_nufft",
+           "type3_nufft_naive"]
 
 
 @dataclass
@@ -211,6 +212,60 @@ class type3_nufft(linop):
         return xo.reshape((N, *self.ishape))
 
 
+class _LowRankPlan:
+    """Components j = (k, l) of a low-rank SENSE model, k a subspace
+    coefficient (image k) and l a segment (spatial function b_l), on one
+    multi-slice plan whose slices share the trajectory (mrn_lr_forward /
+    mrn_lr_adjoint / mrn_lr_normal). Components are ordered k-major, so
+    the image-side sums over segments are one reshape and sum in a fixed
+    order. ``weights`` (K, L, M) holds the temporal weight of each component
+    (phi_k(t) h_l(t)); ``spatial`` (L, *im) the b_l."""
+
+    def __init__(self, nufft: b200_nufft, trj, mps, dcf, spatial, weights):
+        K, L, M = weights.shape
+        im = tuple(mps.shape[1:])
+        C = mps.shape[0]
+        d = trj.shape[-1]
+        J = K * L
+        dev = trj.device
+        self.K, self.L, self.J, self.im, self.C, self.M = K, L, J, im, C, M
+        self.plan = Plan([im] * J, [M] * J, [C] * J, nufft.oversamp, nufft._widths(), nufft.beta,
+                         apodize=nufft.apodize, tile=nufft.tile, coil_group=nufft.coil_group,
+                         max_chunk=nufft.max_chunk, device=dev, fast=nufft.fast,
+                         warp_grid=nufft.warp_grid, weight_tables=nufft.weight_tables,
+                         reg_grid=nufft.reg_grid, reg_interp=nufft.reg_interp)
+        self.plan.set_traj(trj.reshape(1, M, d).expand(J, M, d).contiguous().reshape(-1))
+        self.mps = mps.to(complex_dtype).reshape(1, -1).expand(J, -1).contiguous().reshape(-1)
+        self.w_fwd = weights.to(complex_dtype).reshape(J, M).contiguous()
+        self.w_adj = (self.w_fwd * dcf.reshape(1, M).to(real_dtype)).contiguous()
+        self.b = spatial.to(complex_dtype).reshape(L, -1).contiguous()
+
+    def _components(self, alphas):
+        """(K, *im) coefficient images -> (K*L, N) component images b_l alpha_k."""
+        a = alphas.to(complex_dtype).reshape(self.K, 1, -1)
+        return (a * self.b[None]).reshape(self.J, -1).contiguous()
+
+    def _gather(self, xc):
+        """(K*L, N) component images -> (K, N): sum_l conj(b_l) x_(k,l)."""
+        return (xc.reshape(self.K, self.L, -1) * self.b.conj()[None]).sum(1)
+
+    def forward(self, alphas):
+        ksp = torch.empty((self.C, self.M), dtype=complex_dtype, device=alphas.device)
+        self.plan.lr_forward(self._components(alphas), self.mps, self.w_fwd, ksp)
+        return ksp
+
+    def adjoint(self, ksp):
+        xc = torch.empty((self.J, self.b.shape[1]), dtype=complex_dtype, device=ksp.device)
+        self.plan.lr_adjoint(ksp.to(complex_dtype).contiguous(), self.w_adj, self.mps, xc)
+        return self._gather(xc)
+
+    def normal(self, alphas):
+        xc = self._components(alphas)
+        out = torch.empty_like(xc)
+        self.plan.lr_normal(xc, self.mps, self.w_fwd, self.w_adj, out)
+        return self._gather(out)
+
+
 class sense_linop(linop):
     """SENSE model y_c = sum_l h_l * F(S_c * b_l * x) (linops.py:1041-1308)."""
 
@@ -278,6 +333,14 @@ class sense_linop(linop):
                 and not trj.requires_grad):
             self.seg = self._segment_plan(nufft, trj, mps, dcf, spatial_funcs, temporal_funcs)
 
+        # any other segmentation (least-squares interpolators, linops.py:1151-1176,
+        # 1196-1226): every segment is one component of a low-rank plan, the
+        # temporal weights applied in the fused combine / gridding prologue
+        self.lr = None
+        if (isinstance(nufft, b200_nufft) and self.segmented and self.seg is None
+                and not use_toeplitz and not trj.requires_grad):
+            self.lr = self._lowrank_plan(nufft, trj, mps, dcf, spatial_funcs, temporal_funcs)
+
         if use_toeplitz:
             # linops.py:1102-1119: the spatial/temporal defaults are already in
             # place here, so the reference always builds (L, L, *im_os) kernels
@@ -333,6 +396,28 @@ class sense_linop(linop):
                 "dcf": dcf.reshape(M)[order].contiguous(),
                 "b": spatial.to(complex_dtype).reshape(L, -1).contiguous()}
 
+    def _lowrank_plan(self, nufft, trj, mps, dcf, spatial, temporal):
+        """Low-rank plan of L segments (K = 1), or None when the shapes do
+        not broadcast to one spatial function and one temporal weight per
+        segment."""
+        L = max(spatial.shape[0], temporal.shape[0])
+        im, ts = self.im_size, self.trj_size
+        try:
+            sp = spatial.to(complex_dtype).expand((L, *im))
+            tf = temporal.to(complex_dtype).expand((L, *ts))
+        except RuntimeError:
+            return None
+        M = 1
+        for v in ts:
+            M *= int(v)
+        return _LowRankPlan(nufft, trj.reshape(M, trj.shape[-1]), mps, dcf, sp,
+                            tf.reshape(1, L, M))
+
+    def _use_lr(self, *tensors):
+        if self.lr is None:
+            return False
+        return not (torch.is_grad_enabled() and any(t.requires_grad for t in tensors))
+
     def _use_seg(self, *tensors):
         if self.seg is None:
             return False
@@ -346,6 +431,8 @@ class sense_linop(linop):
             kp = torch.empty(sg["plan"].n_ksp, dtype=complex_dtype, device=img.device)
             sg["plan"].sense_forward(xl, sg["mps"], kp)
             return kp[sg["src"]].reshape((self.mps.shape[0], *self.trj_size))
+        if self._use_lr(img):
+            return self.lr.forward(img.reshape(1, *self.im_size)).reshape((self.mps.shape[0], *self.trj_size))
         if self.plan is not None:
             x = img.to(complex_dtype).contiguous()
             ksp = torch.empty((self.mps.shape[0], *self.trj_size), dtype=complex_dtype, device=x.device)
@@ -370,6 +457,8 @@ class sense_linop(linop):
             xl = torch.empty_like(sg["b"])
             sg["plan"].sense_adjoint(kp, sg["dcf"], sg["mps"], xl)
             return (sg["b"].conj() * xl).sum(0).reshape(self.im_size)
+        if self._use_lr(ksp):
+            return self.lr.adjoint(ksp.reshape(self.mps.shape[0], -1)).reshape(self.im_size)
         if self.plan is not None:
             y = ksp.to(complex_dtype).contiguous()
             img = torch.empty(self.im_size, dtype=complex_dtype, device=y.device)
@@ -394,6 +483,8 @@ class sense_linop(linop):
                 out = torch.empty_like(xl)
                 sg["plan"].sense_normal(xl, sg["mps"], sg["dcf"], out)
                 return (sg["b"].conj() * out).sum(0).reshape(self.im_size)
+            if self._use_lr(img):
+                return self.lr.normal(img.reshape(1, *self.im_size)).reshape(self.im_size)
             if self.plan is not None:
                 x = img.to(complex_dtype).contiguous()
                 out = torch.empty_like(x)
@@ -420,3 +511,168 @@ class sense_linop(linop):
             y = (y * self.spatial_funcs[m1:m2].conj()).sum(dim=-dim - 1)
             img_hat += (y * self.mps.conj()).sum(dim=0)
         return img_hat
+
+
+def _subspace_weights(phi, temporal, trj_size):
+    """(K, L, M) component weights phi_k(t) h_l(t); phi (K, T) runs along the
+    last trajectory dimension (linops.py:1640, 'nsub ntr')."""
+    K = phi.shape[0]
+    L = temporal.shape[0]
+    ts = tuple(trj_size)
+    ph = phi.to(complex_dtype).reshape((K,) + (1,) * (len(ts) - 1) + (ts[-1],)).expand((K, *ts))
+    tf = temporal.to(complex_dtype).expand((L, *ts))
+    return (ph[:, None] * tf[None]).reshape(K, L, -1)
+
+
+class subspace_linop(linop):
+    """Subspace model y_c = sum_k phi_k(t) sum_l h_l(t) F(S_c b_l alpha_k)
+    (linops.py:1496-1772): alphas (nsub, *im_size) -> ksp (C, *trj_size),
+    phi (nsub, ntr) along the last trajectory dimension. With the B200 NUFFT
+    every (coefficient, segment) pair is one component of a low-rank plan
+    (mrn_lr_*): one pre / FFT / interpolation pass over all components with
+    the phi_k h_l weights summed in a fused combine, and a gridding that
+    reads the k-space once per component with conj(phi_k h_l) dcf applied
+    in its prologue, where the reference loops over coil, segment and
+    subspace batches (linops.py:1613-1700). The Toeplitz normal follows
+    linops.py:1703-1772 on the B200 kernels' PSFs."""
+
+    def __init__(self, im_size: tuple, trj: torch.Tensor, mps: torch.Tensor, phi: torch.Tensor,
+                 dcf: Optional[torch.Tensor] = None, nufft: Optional[NUFFT] = None,
+                 use_toeplitz: Optional[bool] = False, spatial_funcs: Optional[torch.Tensor] = None,
+                 temporal_funcs: Optional[torch.Tensor] = None,
+                 bparams: Optional[batching_params] = batching_params()):
+        im_size = tuple(im_size)
+        ishape = (phi.shape[0], *im_size)
+        oshape = (mps.shape[0], *trj.shape[:-1])
+        super().__init__(ishape, oshape)
+        dev = trj.device
+        assert phi.device == dev and mps.device == dev
+        _lib.require_cuda(trj, "trajectory")
+        if nufft is None:
+            nufft = b200_nufft(im_size)
+        trj_size = tuple(trj.shape[:-1])
+        if dcf is None:
+            dcf = torch.ones(trj_size, dtype=real_dtype, device=dev)
+        if spatial_funcs is None:
+            spatial_funcs = torch.ones((1,) * len(ishape), dtype=complex_dtype, device=dev)
+        if temporal_funcs is None:
+            temporal_funcs = torch.ones((1,) * len(oshape), dtype=complex_dtype, device=dev)
+        trj = nufft.rescale_trajectory(trj).type(real_dtype)
+        dcf = dcf.type(real_dtype)
+        mps = mps.type(complex_dtype)
+        phi = phi.type(complex_dtype)
+        self.im_size = im_size
+        self.trj_size = trj_size
+        self.use_toeplitz = use_toeplitz
+        self.trj, self.phi, self.mps, self.dcf = trj, phi, mps, dcf
+        self.nufft = nufft
+        self.bparams = bparams
+        self.torch_dev = dev
+        self.spatial_funcs = spatial_funcs
+        self.temporal_funcs = temporal_funcs
+
+        self.toep_kerns = None
+        if use_toeplitz:
+            # linops.py:1581-1601: kernels for every (nsub1, nsub2) pair of the
+            # weights conj(phi_1) phi_2 dcf
+            if spatial_funcs.numel() > 1:
+                raise NotImplementedError("Toeplitz subspace model with spatial functions")
+            K = phi.shape[0]
+            phis = phi.conj()[:, None, :] * phi[None, ...]
+            w = rearrange(phis, "k1 k2 ntr -> (k1 k2) ntr")
+            w = w.reshape((K * K,) + (1,) * (len(trj_size) - 1) + (trj_size[-1],)) * dcf
+            kerns = [nufft.calc_teoplitz_kernels(trj[None], w[a:a + 1]) for a in range(K * K)]
+            self.toep_kerns = rearrange(torch.cat(kerns, 0), "(k1 k2) ... -> k1 k2 ...", k1=K, k2=K)
+
+        self.lr = None
+        if isinstance(nufft, b200_nufft) and not use_toeplitz and not trj.requires_grad:
+            L = max(spatial_funcs.shape[0], temporal_funcs.shape[0])
+            sp = spatial_funcs.to(complex_dtype).expand((L, *im_size))
+            wts = _subspace_weights(phi, temporal_funcs.expand((L, *trj_size)), trj_size)
+            self.lr = _LowRankPlan(nufft, trj.reshape(-1, trj.shape[-1]), mps, dcf, sp, wts)
+
+    def _use_lr(self, *tensors):
+        if self.lr is None:
+            return False
+        return not (torch.is_grad_enabled() and any(t.requires_grad for t in tensors))
+
+    def forward(self, alphas: torch.Tensor) -> torch.Tensor:
+        """(nsub, *im_size) -> (C, *trj_size) (linops.py:1613-1655)."""
+        if self._use_lr(alphas):
+            return self.lr.forward(alphas).reshape(self.oshape)
+        nc = self.mps.shape[0]
+        ksp = torch.zeros((nc, *self.trj_size), dtype=complex_dtype, device=self.torch_dev)
+        L = self.spatial_funcs.shape[0]
+        for l1, l2 in batch_iterator(L, L):
+            mw = self.mps[:, None] * self.spatial_funcs[l1:l2]
+            Sx = einsum(mw, alphas.to(complex_dtype), "nc nseg ..., nsub ... -> nc nsub nseg ...")
+            FSx = self.nufft.forward(Sx[None], self.trj[None])[0]  # nc nsub nseg *trj
+            ph = self.phi.reshape((self.phi.shape[0], 1) + (1,) * (len(self.trj_size) - 1) + (self.trj_size[-1],))
+            PFSx = (FSx * ph[None]).sum(1)  # nc nseg *trj
+            ksp += (PFSx * self.temporal_funcs[l1:l2]).sum(1)
+        return ksp
+
+    def adjoint(self, ksp: torch.Tensor) -> torch.Tensor:
+        """(C, *trj_size) -> (nsub, *im_size) (linops.py:1657-1700)."""
+        if self._use_lr(ksp):
+            return self.lr.adjoint(ksp.reshape(self.mps.shape[0], -1)).reshape(self.ishape)
+        L = self.spatial_funcs.shape[0]
+        kw = ksp.to(complex_dtype) * self.dcf[None]
+        alphas = torch.zeros(self.ishape, dtype=complex_dtype, device=self.torch_dev)
+        ph = self.phi.conj().reshape((self.phi.shape[0], 1) + (1,) * (len(self.trj_size) - 1) + (self.trj_size[-1],))
+        for l1, l2 in batch_iterator(L, L):
+            Wy = kw[:, None] * self.temporal_funcs[l1:l2].conj()  # nc nseg *trj
+            PWy = Wy[:, None] * ph[None]  # nc nsub nseg *trj
+            FPWy = self.nufft.adjoint(PWy[None], self.trj[None])[0]  # nc nsub nseg *im
+            SF = einsum(FPWy, self.mps.conj(), "nc nsub nseg ..., nc ... -> nsub nseg ...")
+            alphas += (SF * self.spatial_funcs[l1:l2].conj()).sum(1)
+        return alphas
+
+    def normal(self, alphas: torch.Tensor) -> torch.Tensor:
+        """A^H A alphas (linops.py:1702-1772)."""
+        if not self.use_toeplitz:
+            if self._use_lr(alphas):
+                return self.lr.normal(alphas).reshape(self.ishape)
+            return self.adjoint(self.forward(alphas))
+        dim = len(self.im_size)
+        K = self.phi.shape[0]
+        padder = PadLast(self.toep_kerns.shape[-dim:], self.im_size)
+        Sx = self.mps[:, None] * alphas.to(complex_dtype)[None]  # nc nsub *im
+        FRSx = fft(padder.forward(Sx), dim=tuple(range(-dim, 0)))
+        out = torch.zeros_like(alphas, dtype=complex_dtype)
+        for i in range(K):
+            MF = einsum(self.toep_kerns[i], FRSx, "nsub ..., nc nsub ... -> nc ...")
+            y = padder.adjoint(ifft(MF, dim=tuple(range(-dim, 0))))
+            out[i] = (y * self.mps.conj()).sum(0)
+        return out
+
+
+class subspace_linop_new(linop):
+    """Subspace model over a (segmented) sense_linop (linops.py:1379-1495):
+    trj (*trj_size, d) with trj_size = (..., T), phi (K, T), alphas (K,
+    *im_size). Same operator as ``subspace_linop``; runs on its low-rank
+    plan (one pass over every coefficient and segment)."""
+
+    def __init__(self, trj: torch.Tensor, mps: torch.Tensor, phi: torch.Tensor,
+                 dcf: Optional[torch.Tensor] = None, nufft: Optional[NUFFT] = None,
+                 use_toeplitz: Optional[bool] = False, spatial_funcs: Optional[torch.Tensor] = None,
+                 temporal_funcs: Optional[torch.Tensor] = None,
+                 bparams: Optional[batching_params] = batching_params()):
+        im_size = tuple(mps.shape[1:])
+        super().__init__((phi.shape[0], *im_size), (mps.shape[0], *trj.shape[:-1]))
+        if use_toeplitz is True:
+            raise NotImplementedError("Toeplitz normal operator not implemented for subspace models")
+        assert phi.shape[1] == trj.shape[-2]
+        self.phi = phi
+        self.A = subspace_linop(im_size, trj, mps, phi, dcf=dcf, nufft=nufft, use_toeplitz=False,
+                                spatial_funcs=spatial_funcs, temporal_funcs=temporal_funcs,
+                                bparams=bparams)
+
+    def forward(self, alphas: torch.Tensor) -> torch.Tensor:
+        return self.A.forward(alphas)
+
+    def adjoint(self, ksp: torch.Tensor) -> torch.Tensor:
+        return self.A.adjoint(ksp)
+
+    def normal(self, alphas: torch.Tensor) -> torch.Tensor:
+        return self.A.normal(alphas)

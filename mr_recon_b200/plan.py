@@ -168,6 +168,18 @@ class Plan:
         self._call("mrn_sense_normal", ptr(x), ptr(mps), ptr(dcf), ptr(out), float(out_scale),
                    float(lam), ptr(pap), int(pap_stride))
 
+    def lr_forward(self, x, mps, w, ksp):
+        """Low-rank forward: ksp = sum_j w[j] * NUFFT_j(mps[j] x[j]) (mrn_lr_forward)."""
+        self._call("mrn_lr_forward", ptr(x), ptr(mps), ptr(w), ptr(ksp))
+
+    def lr_adjoint(self, ksp, w, mps, x, out_scale=1.0):
+        """Low-rank adjoint: x[j] = sum_c conj(mps[j][c]) NUFFT_j^H(conj(w[j]) ksp[c])."""
+        self._call("mrn_lr_adjoint", ptr(ksp), ptr(w), ptr(mps), ptr(x), float(out_scale))
+
+    def lr_normal(self, x, mps, w_fwd, w_adj, out, out_scale=1.0, lam=0.0):
+        self._call("mrn_lr_normal", ptr(x), ptr(mps), ptr(w_fwd), ptr(w_adj), ptr(out),
+                   float(out_scale), float(lam))
+
     def set_toeplitz(self, kern: torch.Tensor, pad_sizes) -> None:
         """Bind Toeplitz kernels (calc_teoplitz_kernels' output, per slice on
         the padded grid pad_sizes[s], slices back to back); see mrn_plan_set_toeplitz."""

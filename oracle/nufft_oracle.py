@@ -548,6 +548,30 @@ class SenseOracle:
         return self.adjoint(self.forward(img))
 
 
+class SubspaceOracle:
+    """subspace_linop (linops.py:1496-1772): alphas (K, *im) -> ksp (C, *T),
+    y_c = sum_k phi_k(t) sum_l h_l(t) F(S_c b_l alpha_k), phi (K, ntr) along
+    the last trajectory dimension; adjoint alpha_k = sum_l conj(b_l) sum_c
+    conj(S_c) F^H(conj(phi_k) conj(h_l) dcf y_c) (linops.py:1657-1700)."""
+
+    def __init__(self, trj, mps, phi, nufft: KBNufftOracle, dcf=None,
+                 spatial_funcs=None, temporal_funcs=None):
+        self.sense = SenseOracle(trj, mps, nufft, dcf, spatial_funcs, temporal_funcs)
+        tshape = self.sense.trj.shape[:-1]
+        phi = np.asarray(phi).astype(C64)
+        self.phi = phi.reshape((phi.shape[0],) + (1,) * (len(tshape) - 1) + (tshape[-1],))
+
+    def forward(self, alphas):  # linops.py:1613-1655
+        out = 0
+        for k in range(self.phi.shape[0]):
+            out = out + self.sense.forward(alphas[k]) * self.phi[k]
+        return np.asarray(out).astype(C64)
+
+    def adjoint(self, ksp):  # linops.py:1657-1700
+        return np.stack([self.sense.adjoint((ksp * np.conj(self.phi[k])).astype(C64))
+                         for k in range(self.phi.shape[0])]).astype(C64)
+
+
 def _vdot_real(a, b):
     return float(np.real(np.vdot(a.astype(np.complex128), b.astype(np.complex128))))
 
