@@ -18,7 +18,8 @@ from typing import Optional, Tuple
 
 import torch
 
-__all__ = ["b0_to_phis_alphas", "alpha_segementation", "uniform_quantize"]
+__all__ = ["b0_to_phis_alphas", "alpha_segementation", "uniform_quantize", "kmeans_quantize",
+           "isotropic_cluster_alphas"]
 
 complex_dtype = torch.complex64
 real_dtype = torch.float32
@@ -52,6 +53,62 @@ def uniform_quantize(data: torch.Tensor, K: int) -> Tuple[torch.Tensor, torch.Te
     return centers.reshape(K, 1), idx.reshape(data.shape[:-1])
 
 
+def kmeans_quantize(data: torch.Tensor, K: int, max_iter: int = 1000,
+                    seed: int = 0) -> Tuple[torch.Tensor, torch.Tensor]:
+    """K cluster centres of data (n, d) and each point's nearest centre, by
+    Lloyd's k-means with euclidean distances (the 'cluster' method of
+    mr_recon's utils.quantize_data, utils.py:117-135, which calls
+    fast_pytorch_kmeans' KMeans(max_iter=1000, mode='euclidean')). The
+    initial centres come from k-means++ seeding with a fixed generator, so
+    the result is the same on every call (KMeans seeds from the global RNG);
+    iterations stop when no assignment changes. A centre that loses all its
+    points keeps its position."""
+    x = data.reshape(data.shape[0], -1).to(torch.float64)
+    n = x.shape[0]
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    first = int(torch.randint(n, (1,), generator=g))
+    cents = [x[first]]
+    d2 = ((x - cents[0]) ** 2).sum(1)
+    for _ in range(1, K):
+        p = (d2 / d2.sum()).cpu() if float(d2.sum()) > 0 else torch.full((n,), 1.0 / n, dtype=torch.float64)
+        i = int(torch.multinomial(p, 1, generator=g))
+        cents.append(x[i])
+        d2 = torch.minimum(d2, ((x - x[i]) ** 2).sum(1))
+    c = torch.stack(cents)
+    idx = torch.cdist(x, c).argmin(1)
+    for _ in range(max_iter):
+        cnt = torch.bincount(idx, minlength=K).to(x.dtype)
+        sums = torch.zeros_like(c).index_add_(0, idx, x)
+        c = torch.where(cnt[:, None] > 0, sums / cnt.clamp(min=1)[:, None], c)
+        new = torch.cdist(x, c).argmin(1)
+        if torch.equal(new, idx):
+            break
+        idx = new
+    return c.to(data.dtype), idx
+
+
+def isotropic_cluster_alphas(alphas: torch.Tensor, phis: torch.Tensor,
+                             L: int) -> Tuple[torch.Tensor, torch.Tensor]:
+    """Segment centres (L, B) and per-sample indices (*trj_size) for several
+    phase bases (field.py:216-269): phis and alphas are centred on their
+    range midpoints, phis scaled to [-1/2, 1/2] per basis and alphas by the
+    inverse, so the k-means distance in alpha space is the same phase error
+    for every basis; the centres are scaled back."""
+    B = alphas.shape[0]
+    trj_size = alphas.shape[1:]
+    ph = phis.reshape(B, -1).to(torch.float64)
+    al = alphas.reshape(B, -1).to(torch.float64)
+    ph_mp = (ph.min(1).values + ph.max(1).values) / 2
+    al_mp = (al.min(1).values + al.max(1).values) / 2
+    ph_c = ph - ph_mp[:, None]
+    al_c = al - al_mp[:, None]
+    scales = ph_c.abs().max(1).values * 2
+    al_c = al_c * scales[:, None]
+    cents, inds = kmeans_quantize(al_c.T.contiguous(), L)
+    cents = cents / scales + al_mp
+    return cents.reshape(L, B), inds.reshape(trj_size)
+
+
 def alpha_segementation(phis: torch.Tensor, alphas: torch.Tensor, L: int,
                         L_batch_size: Optional[int] = 1, interp_type: Optional[str] = "zero",
                         use_type3: Optional[bool] = True,
@@ -74,11 +131,14 @@ def alpha_segementation(phis: torch.Tensor, alphas: torch.Tensor, L: int,
       product instead of a dense R x T matrix).
     ``L_batch_size`` and ``verbose`` are accepted for interface
     compatibility."""
-    if phis.shape[0] != 1 or alphas.shape[0] != 1:
-        raise NotImplementedError("alpha_segementation supports a single phase basis (B = 1)")
+    B = phis.shape[0]
+    if alphas.shape[0] != B:
+        raise ValueError("phis and alphas need the same number of phase bases")
     dev = phis.device
     im_size = phis.shape[1:]
     trj_size = alphas.shape[1:]
+    if B > 1:
+        return _segment_multi(phis, alphas, L, interp_type, use_type3, manual_spatial_funcs)
     cents, inds = uniform_quantize(alphas.moveaxis(0, -1), L)
     a_l = cents[:, 0].to(real_dtype)
     ph = phis[0].to(real_dtype)
@@ -119,3 +179,42 @@ def alpha_segementation(phis: torch.Tensor, alphas: torch.Tensor, L: int,
     else:
         raise NotImplementedError(f"interp_type {interp_type!r}")
     return spatial, temporal
+
+
+def _segment_multi(phis, alphas, L, interp_type, use_type3, manual_spatial_funcs):
+    """alpha_segementation for B > 1 phase bases (field.py:321-369): centres
+    by isotropic k-means, b_l(r) = exp(-2 pi i sum_b phis_b(r) alpha_l,b),
+    'zero' one-hot h_l or the 'lstsq' interpolator from the B-dimensional
+    type-3 NUFFT (B <= 3 on the B200 kernels) or the exact sums."""
+    B = phis.shape[0]
+    im_size = phis.shape[1:]
+    trj_size = alphas.shape[1:]
+    cents, inds = isotropic_cluster_alphas(alphas, phis, L)
+    ph = phis.reshape(B, -1).to(torch.float64)
+    spatial = torch.exp(-2j * math.pi * (cents.to(torch.float64) @ ph)).to(complex_dtype)
+    spatial = spatial.reshape((L, *im_size))
+    if manual_spatial_funcs is not None:
+        spatial = manual_spatial_funcs
+    if "zero" in interp_type:
+        temporal = torch.stack([(inds == l).to(complex_dtype) for l in range(L)], 0)
+        return spatial, temporal
+    if "lstsq" not in interp_type:
+        raise NotImplementedError(f"interp_type {interp_type!r}")
+    n = ph.shape[1]
+    sp = spatial.reshape(L, -1)
+    AHA = (sp.conj() @ sp.T) / n
+    if use_type3:
+        from .linops import type3_nufft
+        t3n = type3_nufft(phis, alphas)
+        AHy = t3n.forward(spatial.conj().to(complex_dtype)).reshape(L, -1) / n
+    else:
+        al = alphas.reshape(B, -1).to(torch.float64)
+        AHy = torch.zeros((L, al.shape[1]), dtype=torch.complex128, device=phis.device)
+        sp64 = sp.to(torch.complex128).conj()
+        chunk = max(1, (1 << 24) // max(n, 1))
+        for c0 in range(0, al.shape[1], chunk):
+            e = torch.exp(-2j * math.pi * (ph.T @ al[:, c0:c0 + chunk]))  # (N, chunk)
+            AHy[:, c0:c0 + chunk] = (sp64 @ e) / n
+        AHA = AHA.to(torch.complex128)
+    h = torch.linalg.pinv(AHA) @ AHy.to(AHA.dtype)
+    return spatial, h.reshape((L, *trj_size)).to(complex_dtype)

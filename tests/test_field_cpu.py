@@ -70,3 +70,51 @@ def test_segmented_phase_model_error_falls_with_L():
         approx = torch.einsum("lxy,lat->xyat", s, t)
         errs.append(rel(approx.numpy(), exact.numpy()))
     assert all(b < a for a, b in zip(errs, errs[1:])) and errs[-1] < 1e-3
+
+
+def test_two_phase_bases_kmeans_segmentation():
+    """B = 2 phase bases (field.py:321-369 with isotropic_cluster_alphas,
+    216-269): the k-means centres are a Lloyd fixed point (every point is
+    assigned to its nearest centre, every centre is the mean of its points,
+    in the isotropically scaled alpha space), the run is deterministic, and
+    the zero-order and least-squares (exact sums) segmentations approximate
+    the phase model better as L grows. The reference's k-means
+    (fast_pytorch_kmeans) seeds from the global RNG, so its centres cannot
+    be fixed as vectors; these properties are what it converges to too."""
+    from mr_recon_b200.field import isotropic_cluster_alphas, kmeans_quantize
+    rng = np.random.RandomState(3)
+    im, T = (24, 20), 300
+    yy, xx = np.meshgrid(np.linspace(-1, 1, im[0]), np.linspace(-1, 1, im[1]), indexing="ij")
+    phis = torch.from_numpy(np.stack([0.4 * xx + 0.1 * yy ** 2, 0.5 * yy]).astype(np.float32))
+    t = np.linspace(0, 1, T)
+    alphas = torch.from_numpy(np.stack([30 * t, 12 * np.sin(3 * t) + rng.randn(T) * 0.2]).astype(np.float32))
+    cents, inds = isotropic_cluster_alphas(alphas, phis, 8)
+    c2, i2 = isotropic_cluster_alphas(alphas, phis, 8)
+    assert torch.equal(cents, c2) and torch.equal(inds, i2)
+    # Lloyd fixed point in the scaled space
+    ph = phis.reshape(2, -1).double()
+    al = alphas.reshape(2, -1).double()
+    sc = (ph - ((ph.min(1).values + ph.max(1).values) / 2)[:, None]).abs().max(1).values * 2
+    amp = (al.min(1).values + al.max(1).values) / 2
+    x = ((al - amp[:, None]) * sc[:, None]).T
+    cs = (cents.double() - amp) * sc
+    assert torch.equal(torch.cdist(x, cs).argmin(1), inds.reshape(-1))
+    for l in range(8):
+        if (inds == l).any():
+            assert torch.allclose(x[inds.reshape(-1) == l].mean(0), cs[l], atol=1e-9)
+    # direct use of the k-means quantiser: a clean three-cluster case
+    pts = torch.cat([torch.randn(50, 2, generator=torch.Generator().manual_seed(1)) * 0.05 + c
+                     for c in (torch.tensor([0., 0.]), torch.tensor([3., 0.]), torch.tensor([0., 3.]))])
+    cc, ii = kmeans_quantize(pts, 3)
+    assert sorted(torch.bincount(ii).tolist()) == [50, 50, 50]
+    # model error falls with L
+    e_true = torch.exp(-2j * np.pi * (ph.T @ al))  # (N, T)
+
+    def err(L, kind):
+        s, tf = alpha_segementation(phis, alphas, L, interp_type=kind, use_type3=False, verbose=False)
+        approx = s.reshape(L, -1).T.to(torch.complex128) @ tf.reshape(L, -1).to(torch.complex128)
+        return float((approx - e_true).norm() / e_true.norm())
+    for kind in ("zero", "lstsq"):
+        errs = [err(L, kind) for L in (3, 6, 12)]
+        assert errs[0] > errs[1] > errs[2]
+    assert err(6, "lstsq") < err(6, "zero")
