@@ -48,10 +48,11 @@ HOST_AHEAD_S = 0.4e-3  # device-side wait before each timed step: longer than th
 # DRAM bytes (read + write) per launch of each tile kernel on this workload,
 # from one ncu capture of the kernels named in TRAFFIC_SOURCE (ncu cannot run
 # inside the timed program, so the figure is carried here and labelled).
-GRID_TRAFFIC_BYTES = 33_565_440 + 60_928
-INTERP_TRAFFIC_BYTES = 26_191_360 + 1_033_728
-TRAFFIC_SOURCE = ("ncu --set full capture of k_grid_reg<6,1> and k_interp_reg<2,7,1> on this workload "
-                  "(dram__bytes_read.sum + dram__bytes_write.sum per launch)")
+GRID_TRAFFIC_BYTES = 30_618_624 + 2_219_264
+INTERP_TRAFFIC_BYTES = 26_141_440 + 982_272
+TRAFFIC_SOURCE = ("ncu --set full capture of k_grid_reg<7,1> (write-back staged through shared memory) "
+                  "and k_interp_reg<2,7,1> on this workload (dram__bytes_read.sum + dram__bytes_write.sum "
+                  "per launch)")
 CG_FIXTURE = os.path.join(ROOT, "tests", "golden", "cg_config2.npz")
 # Speed of the oracle port relative to the reference's own CPU path
 # (triton_nufft on CPU tensors, its torch fallback) on this workload: both
