@@ -250,6 +250,33 @@ def grid(vals, locs, grid_size, width, beta, chunk=1 << 14):
     return out.reshape(*vals.shape[:-1], *grid_size) if vals.ndim > 1 else out.reshape(grid_size)
 
 
+def pipe_menon_dcf(trj, im_size, max_iter=30, beta=8.0, width=4.0):
+    """Pipe-Menon density compensation as the reference's
+    density_compensation(method='sigpy') computes it (algs.py:20-106): it
+    calls sigpy.mri.pipe_menon_dcf(coord, img_shape, max_iter) -- sigpy is a
+    third-party dependency, unpinned in the reference's environment.yml and
+    absent here. Restated from that published routine (Pipe & Menon, MRM
+    41:179-186, 1999): G = sigpy's Kaiser-Bessel gridding of the samples onto
+    the img_shape grid (kernel 'kaiser_bessel', width 4, param beta 8, taps
+    ceil(k - w/2) .. floor(k + w/2), the A&S I0 polynomial -- the same weight
+    and tap rule as the reference's triton_interp, whose kernels.py says it
+    follows sigpy), circular cells; w = 1, then w <- w / |G^H G w| for
+    max_iter iterations; the reference then divides by the maximum. The grid
+    origin (sigpy uses the coordinates as they are, this oracle shifts them
+    by N // 2) only shifts the grid circularly, which G^H G does not see."""
+    trj = np.asarray(trj, dtype=F32)
+    d = trj.shape[-1]
+    tshape = trj.shape[:-1]
+    locs = (trj.reshape(-1, d) + np.array([n // 2 for n in im_size], dtype=F32)).astype(F32)
+    w = np.ones(locs.shape[0], dtype=np.complex128)
+    for _ in range(int(max_iter)):
+        g = grid(w.astype(C64)[None], locs, tuple(im_size), width, beta)
+        ghgw = ungrid(g, locs, width, beta)[0].astype(np.complex128)
+        w = w / np.abs(ghgw)
+    dcf = w.real.reshape(tshape)
+    return (dcf / dcf.max()).astype(F32)
+
+
 # --------------------------------------------------------------------------
 # Centred FFT and resize: fourier.py:37-61, utils.py:41-84
 # --------------------------------------------------------------------------

@@ -522,6 +522,25 @@ def test_density_compensation_pipe_menon_properties():
     assert float(inner) < float(mid) < float(outer)
 
 
+@pytest.mark.parametrize("case", ["radial2d", "spiral2d", "random3d"])
+def test_density_compensation_matches_pipe_menon_oracle(case):
+    """density_compensation (algs.py:20-106) against the oracle's restatement
+    of sigpy.mri.pipe_menon_dcf (the routine the reference calls): the same
+    30 iterations of w <- w / |G^H G w| on the same gridding operator."""
+    from mr_recon_b200.algs import density_compensation
+    rng = np.random.RandomState(11)
+    if case == "radial2d":
+        im, trj = (48, 48), synth.golden_angle_radial(40, 96, 24.0)
+    elif case == "spiral2d":
+        im, trj = (40, 44), synth.vd_spiral(5, 400, 20.0)
+    else:
+        im = (14, 16, 12)
+        trj = ((rng.rand(3000, 3) - 0.5) * np.array(im)).astype(np.float32)
+    dcf = density_compensation(T(trj), im, num_iters=30)
+    ref = O.pipe_menon_dcf(trj, im, max_iter=30)
+    assert rel(Nn(dcf), ref) < 1e-4
+
+
 # ----------------------------------------------------------------- type-3 NUFFT
 def test_raw_grid_per_axis_beta_matches_oracle():
     """Gridding / interpolation with one KB beta per axis (sigpy's per-axis
@@ -584,6 +603,28 @@ def test_alpha_segmentation_lstsq_type3_vs_exact():
             assert rel(Nn(t3), Nn(te)) < 1e-3
         m3 = rel(np.einsum("lxy,lat->xyat", Nn(s3), Nn(t3)), exact)
         me = rel(np.einsum("lxy,lat->xyat", Nn(se), Nn(te)), exact)
+        assert m3 < me * 1.05 + 2e-3
+
+
+def test_two_basis_segmentation_lstsq_type3_vs_exact():
+    """Two phase bases (field.py:321-369): the least-squares temporal
+    functions through the 2-D type-3 NUFFT agree with the exact voxel sums
+    for a well-conditioned segmentation, and the phase model error of both
+    is within the type-3 accuracy of each other."""
+    from mr_recon_b200.field import alpha_segementation
+    im = (28, 24)
+    yy, xx = np.meshgrid(np.linspace(-1, 1, im[0]), np.linspace(-1, 1, im[1]), indexing="ij")
+    phis = T(np.stack([0.45 * xx + 0.05 * yy ** 2, 0.5 * yy]).astype(np.float32))
+    tt = np.linspace(0, 1, 240)
+    alphas = T(np.stack([25 * tt, 10 * np.sin(2.5 * tt)]).astype(np.float32))
+    exact = np.exp(-2j * np.pi * np.einsum("bxy,bt->xyt", Nn(phis).astype(np.float64), Nn(alphas).astype(np.float64)))
+    for L in (4, 8):
+        s3, t3 = alpha_segementation(phis, alphas, L, interp_type="lstsq", use_type3=True, verbose=False)
+        se, te = alpha_segementation(phis, alphas, L, interp_type="lstsq", use_type3=False, verbose=False)
+        if L == 4:
+            assert rel(Nn(t3), Nn(te)) < 1e-3
+        m3 = rel(np.einsum("lxy,lt->xyt", Nn(s3), Nn(t3)), exact)
+        me = rel(np.einsum("lxy,lt->xyt", Nn(se), Nn(te)), exact)
         assert m3 < me * 1.05 + 2e-3
 
 
