@@ -387,11 +387,21 @@ def bench_c4(dev, iters=30, seed=4, n_slices=64, world=1, rank=0):
     }
     if world > 1:
         return out
-    # per-slice loop on the same kernels: one plan and one eager solve per slice
+    # per-slice loop on the same kernels: one plan and one eager solve per slice,
+    # with the batched plan's tiles, work-item sizes and gridding lane group,
+    # so every slice is computed in the same order as inside the batch
+    from mr_recon_b200 import _lib
     ksp_off = [int(o) for o in plan.ksp_off]
+    maxc = int(max(coils))
+    lanes = 8 if maxc <= 8 else (16 if maxc <= 16 else 32)
     singles = []
     for s in range(n_slices):
         p1 = Plan([ims[s]], [int(npts[s])], [int(coils[s])], 1.25, (6.0, 6.0), device=dev)
+        p1.set_option(_lib.MRN_OPT_INTERP_TILE, int(tune["interp_tile"]))
+        p1.set_option(_lib.MRN_OPT_INTERP_CHUNK, int(tune["interp_chunk"]))
+        p1.set_option(_lib.MRN_OPT_GRID_TILE, int(tune["grid_tile"]))
+        p1.set_option(_lib.MRN_OPT_GRID_CHUNK, int(tune["grid_chunk"]))
+        p1.set_option(_lib.MRN_OPT_GRID_LANES, lanes)
         p1.set_traj(t_t[int(plan.trj_off[s]) // 2:int(plan.trj_off[s]) // 2 + int(npts[s])])
         s1 = SenseCG(p1, m_s[img_off[s]:img_off[s] + nimg[s]], None, iters, 1e-3, 1.0)
         s1.ksp.copy_(ksp[ksp_off[s]:ksp_off[s] + int(coils[s]) * int(npts[s])])

@@ -119,6 +119,13 @@ int mrn_plan_stats(mrn_plan* plan, int64_t* out4);
  * coil over the tile region staged as [cell][coil] (packed two-lane FMAs); 0
  * uses the coil-plane kernel. */
 #define MRN_OPT_REG_INTERP 9
+/* MRN_OPT_GRID_LANES (default 0): lanes of one coil group in the 2D
+ * register gridding, 8, 16 or 32 (0: the plan's coil group rounded up). A
+ * group of fewer lanes than 32 splits a warp into entry streams whose partial
+ * tiles are added at the end, so the summation order depends on it; a
+ * one-slice plan given the lane count of a larger uneven plan (the lanes its
+ * widest slice needs) adds every cell in the same order as that plan. */
+#define MRN_OPT_GRID_LANES 10
 int mrn_plan_set_option(mrn_plan* plan, int option, int value);
 
 /* Kaiser-Bessel beta per dimension for a raw (MRN_PLAN_RAW) plan, beta[0..ndim),

@@ -36,6 +36,7 @@ MRN_OPT_INTERP_TILE = 6
 MRN_OPT_GRID_TILE = 7
 MRN_OPT_REG_GRIDDING = 8
 MRN_OPT_REG_INTERP = 9
+MRN_OPT_GRID_LANES = 10
 
 _vp = C.c_void_p
 _i = C.c_int

@@ -1,7 +1,9 @@
 // Conjugate-gradient vector steps for a batch of independent systems, one
 // image per slice (the loop body of conjugate_gradient, algs.py:779-872).
 // Vectors are complex64; every dot product and norm is a float64 sum in a
-// fixed order (block partials added in block order by the last block), and
+// fixed order that depends on the slice's own length alone (chunk partials
+// added in chunk order by the last block, whatever the launch's grid and
+// whatever other slices share the plan), and
 // the per-slice scalars never leave the device, so a solve can be captured in
 // a CUDA graph (the reference calls .item() every iteration, algs.py:845) and
 // replays to the same bits as the eager solve. State per slice, float64[8]:
@@ -29,25 +31,56 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return t;  // valid in thread 0
 }
 
-// Per-slice float64 sums of the CG kernels: each block stores its partial in
-// part[slice][block]; the last block to arrive adds each slice's partials in
-// block order (one warp per slice) and adds the total to out[slice * stride],
-// skipping slices whose state says done when `state` is given. The result
-// is the same on every run, eager or replayed from a graph.
-__device__ __forceinline__ void slice_sums(double acc, double* __restrict__ part,
+// A slice of n elements is summed in chunks of chunk_len(n) elements (a
+// multiple of kCgChunk, at most kMaxRedBlocks chunks): chunk c is reduced by
+// one block (thread t takes elements c * len + t + k * kCgThreads, then a
+// fixed tree), its partial goes to part[slice][c], and the last block adds
+// the partials in chunk order. Which block takes a chunk does not matter, so
+// the sums are the same for any grid and any other slices in the plan.
+constexpr int kCgChunk = kCgThreads * 4;
+
+__device__ __forceinline__ int64_t chunk_len(int64_t n) {
+  const int64_t span = (int64_t)kCgChunk * kMaxRedBlocks;
+  return (int64_t)kCgChunk * max((n + span - 1) / span, (int64_t)1);
+}
+
+__device__ __forceinline__ int64_t chunk_count(int64_t n) {
+  const int64_t len = chunk_len(n);
+  return (n + len - 1) / len;
+}
+
+// The last block adds each slice's chunk partials in chunk order (one warp
+// per slice) and adds the total to out[slice * stride], skipping slices whose
+// state says done when `state` is given. The result is the same on every
+// run, eager or replayed from a graph.
+__device__ __forceinline__ void slice_sums(const SliceGeom* __restrict__ sl, double* __restrict__ part,
                                            unsigned* __restrict__ counter, double* __restrict__ out,
                                            int stride, const double* __restrict__ state) {
-  const int s = blockIdx.y, nb = gridDim.x, ns = gridDim.y;
-  if (threadIdx.x == 0) part[(int64_t)s * nb + blockIdx.x] = acc;
-  if (!arrive_last_block(counter, (unsigned)(nb * ns))) return;
+  const int ns = gridDim.y;
+  if (!arrive_last_block(counter, (unsigned)(gridDim.x * ns))) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int q = warp; q < ns; q += kCgThreads / 32) {
     if (state && state[q * 8 + 3] != 0.0) continue;
-    const double v = warp_sum_fixed(part + (int64_t)q * nb, nb, lane);
+    const double v = warp_sum_fixed(part + (int64_t)q * kMaxRedBlocks, chunk_count(sl[q].nimg), lane);
     if (lane == 0) out[(int64_t)q * stride] += v;
   }
   __syncthreads();
   if (threadIdx.x == 0) *counter = 0u;
+}
+
+// Chunk loop of one block over its slice: body(k) for every element k of the
+// chunk (global index), then the chunk's float64 partial into part.
+template <class Body>
+__device__ __forceinline__ void chunk_loop(const SliceGeom& g, int s, double* __restrict__ part,
+                                           double* red, Body body) {
+  const int64_t len = chunk_len(g.nimg), nch = chunk_count(g.nimg);
+  for (int64_t c = blockIdx.x; c < nch; c += gridDim.x) {
+    const int64_t e1 = min((c + 1) * len, g.nimg);
+    double acc = 0.0;
+    for (int64_t i = c * len + threadIdx.x; i < e1; i += kCgThreads) acc += body(g.x_off + i);
+    acc = block_sum(acc, red);
+    if (threadIdx.x == 0) part[(int64_t)s * kMaxRedBlocks + c] = acc;
+  }
 }
 
 // r = b - Ab; p = r; x = b; state[0] += |r|^2; state[4] = tol^2
@@ -58,20 +91,16 @@ k_cg_init(const SliceGeom* __restrict__ sl, const float2* __restrict__ b, const 
   __shared__ double red[kCgThreads / 32];
   const int s = blockIdx.y;
   const SliceGeom& g = sl[s];
-  double acc = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < g.nimg;
-       i += (int64_t)gridDim.x * kCgThreads) {
-    const int64_t k = g.x_off + i;
+  chunk_loop(g, s, part, red, [&](int64_t k) {
     const float2 bb = b[k], ab = Ab[k];
     const float2 rr = make_float2(bb.x - ab.x, bb.y - ab.y);
     r[k] = rr;
     p[k] = rr;
     x[k] = bb;
-    acc += (double)rr.x * rr.x + (double)rr.y * rr.y;
-  }
-  acc = block_sum(acc, red);
+    return (double)rr.x * rr.x + (double)rr.y * rr.y;
+  });
   if (threadIdx.x == 0 && blockIdx.x == 0) state[s * 8 + 4] = tol2;
-  slice_sums(acc, part, counter, state + 0, 8, nullptr);
+  slice_sums(sl, part, counter, state + 0, 8, nullptr);
 }
 
 // alpha = rz / pAp; x += alpha p; r -= alpha Ap; state[2] += |r|^2 (skipped when done)
@@ -83,12 +112,9 @@ k_cg_step(const SliceGeom* __restrict__ sl, float2* __restrict__ x, float2* __re
   const int s = blockIdx.y;
   const SliceGeom& g = sl[s];
   const double* S = state + s * 8;
-  double acc = 0.0;
-  if (S[3] == 0.0) {
+  if (S[3] == 0.0) {  // uniform over the block: the whole slice is done or not
     const float alpha = (float)(S[0] / S[1]);
-    for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < g.nimg;
-         i += (int64_t)gridDim.x * kCgThreads) {
-      const int64_t k = g.x_off + i;
+    chunk_loop(g, s, part, red, [&](int64_t k) {
       const float2 pp = p[k], ap = Ap[k];
       float2 xx = x[k], rr = r[k];
       xx.x = fmaf(alpha, pp.x, xx.x);
@@ -97,11 +123,10 @@ k_cg_step(const SliceGeom* __restrict__ sl, float2* __restrict__ x, float2* __re
       rr.y = fmaf(-alpha, ap.y, rr.y);
       x[k] = xx;
       r[k] = rr;
-      acc += (double)rr.x * rr.x + (double)rr.y * rr.y;
-    }
+      return (double)rr.x * rr.x + (double)rr.y * rr.y;
+    });
   }
-  acc = block_sum(acc, red);
-  slice_sums(acc, part, counter, state + 2, 8, state);
+  slice_sums(sl, part, counter, state + 2, 8, state);
 }
 
 // done |= rr < tol^2; beta = rr / rz; p = r + beta p; then (last block) rz = rr,
@@ -152,22 +177,21 @@ k_cg_dot(const SliceGeom* __restrict__ sl, const float2* __restrict__ a, const f
   __shared__ double red[kCgThreads / 32];
   const int s = blockIdx.y;
   const SliceGeom& g = sl[s];
-  double acc = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < g.nimg;
-       i += (int64_t)gridDim.x * kCgThreads) {
-    const int64_t k = g.x_off + i;
+  chunk_loop(g, s, part, red, [&](int64_t k) {
     const float2 aa = a[k], bb = b[k];
-    acc += (double)aa.x * bb.x + (double)aa.y * bb.y;
-  }
-  acc = block_sum(acc, red);
-  slice_sums(acc, part, counter, out, 1, nullptr);
+    return (double)aa.x * bb.x + (double)aa.y * bb.y;
+  });
+  slice_sums(sl, part, counter, out, 1, nullptr);
 }
 
+// One block per chunk of the longest slice (the reductions' order does not
+// depend on this choice).
 static dim3 cg_grid(const mrn_plan* P) {
   int64_t mx = 1;
   for (const auto& g : P->h_slices) mx = std::max<int64_t>(mx, g.nimg);
-  int64_t bx = (mx + kCgThreads * 4 - 1) / (kCgThreads * 4);
-  bx = std::min<int64_t>(std::max<int64_t>(bx, 1), kMaxRedBlocks);
+  const int64_t span = (int64_t)kCgChunk * kMaxRedBlocks;
+  const int64_t len = (int64_t)kCgChunk * std::max<int64_t>((mx + span - 1) / span, 1);
+  const int64_t bx = std::min<int64_t>(std::max<int64_t>((mx + len - 1) / len, 1), kMaxRedBlocks);
   return dim3((unsigned)bx, (unsigned)P->nslices);
 }
 

@@ -293,6 +293,7 @@ struct mrn_plan {
   bool warp_grid = true;  // 2D gridding with warp-private tiles (no atomics) where it applies
   bool reg_grid = true;   // ... with the tile accumulator in registers (tiles <= 8x8)
   bool reg_interp = true;  // 2D interpolation with lane = coil over a [cell][coil] region
+  int grid_lanes = 0;      // 2D register gridding: lanes per coil group (0 = from the coil group)
   int coil_group = 1;      // coils per CTA chosen at plan creation (informational)
   int coil_group_req = 0;  // caller's coil group, 0 = choose per kernel kind
   int max_coil = 1;

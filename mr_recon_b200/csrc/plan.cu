@@ -705,6 +705,10 @@ int mrn_plan_set_option(mrn_plan* P, int option, int value) {
     case MRN_OPT_WEIGHT_TABLES: P->use_wtab = value != 0; return MRN_OK;
     case MRN_OPT_REG_GRIDDING: P->reg_grid = value != 0; return MRN_OK;
     case MRN_OPT_REG_INTERP: P->reg_interp = value != 0; return MRN_OK;
+    case MRN_OPT_GRID_LANES:
+      if (value != 0 && value != 8 && value != 16 && value != 32) return MRN_ERR_ARG;
+      P->grid_lanes = value;
+      return MRN_OK;
     case MRN_OPT_INTERP_CHUNK:
     case MRN_OPT_GRID_CHUNK:
       if (value < 1) return MRN_ERR_ARG;

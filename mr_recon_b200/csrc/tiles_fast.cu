@@ -1316,8 +1316,10 @@ int launch_grid_reg(mrn_plan* P, const float2* ksp, const float* dcf, const floa
   cg = std::max(1, std::min(cg, 32));
   const int ng = (P->max_coil + cg - 1) / cg;
   cg = (P->max_coil + ng - 1) / ng;
-  // entry streams per warp: 32 lanes / (coil group rounded up to 8, 16 or 32)
-  const int sub = cg <= 8 ? 4 : (cg <= 16 ? 2 : 1);
+  // entry streams per warp: 32 lanes / (coil group rounded up to 8, 16 or 32,
+  // or the lane count the plan option asks for when that is larger)
+  const int lanes = std::max(cg, P->grid_lanes);
+  const int sub = lanes <= 8 ? 4 : (lanes <= 16 ? 2 : 1);
   const dim3 gdim((unsigned)P->n_items_grid, (unsigned)ng);
   const int K = P->kb.ntaps[0];
 #define MRN_REG_LAUNCH(KK, SS)                                                              \

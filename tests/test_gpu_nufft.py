@@ -440,6 +440,56 @@ def test_uneven_multislice_plan_matches_per_slice_oracle():
         assert rel(bo, br) < TOL
 
 
+def test_uneven_batched_cg_equals_per_slice_solves_bitwise():
+    """CG-SENSE of an uneven batch (sizes, coil and sample counts differ, a
+    dense spiral centre so gridding tiles split) in one plan against one plan
+    and solve per slice with the batch's tiles, work-item sizes and gridding
+    lane group: the same bits. The CG sums depend on each slice's own length
+    and cuFFT does not depend on the batch count, so nothing else differs."""
+    from mr_recon_b200 import _lib
+    from mr_recon_b200.algs import SenseCG
+    rng = np.random.RandomState(31)
+    sizes = [(48, 48), (64, 64), (40, 40), (56, 56), (64, 64)]
+    coils = [3, 12, 1, 7, 20]
+    npts = [1600, 4800, 800, 3200, 4000]
+    trjs = [synth.vd_spiral(8, m // 8, s[0] / 2.0).reshape(-1, 2) for s, m in zip(sizes, npts)]
+    xs = [synth.ellipse_phantom(s, 6, rng).astype(np.complex64).reshape(-1) for s in sizes]
+    mps = [synth.gaussian_coil_maps(s, c).astype(np.complex64).reshape(-1) for s, c in zip(sizes, coils)]
+    opts = {_lib.MRN_OPT_INTERP_TILE: 10, _lib.MRN_OPT_INTERP_CHUNK: 128,
+            _lib.MRN_OPT_GRID_TILE: 8, _lib.MRN_OPT_GRID_CHUNK: 96}
+
+    def make(ims, ms, cs, trj):
+        p = Plan(ims, ms, cs, 1.25, (6.0, 6.0), device=DEV)
+        for k, v in opts.items():
+            p.set_option(k, v)
+        return p
+
+    plan = make(sizes, npts, coils, np.concatenate(trjs))
+    plan.set_traj(T(np.concatenate(trjs).reshape(-1)))
+    assert plan.stats()["split_tiles"] > 0
+    m_t = T(np.concatenate(mps))
+    ksp = torch.empty(plan.n_ksp, dtype=torch.complex64, device=DEV)
+    plan.sense_forward(T(np.concatenate(xs)), m_t, ksp)
+    ksp += T(synth.randn_complex((plan.n_ksp,), rng)) * 0.01 * float(ksp.abs().max())
+    cg = SenseCG(plan, m_t, None, 12, 1e-3, 40.0)
+    cg.ksp.copy_(ksp)
+    xb = cg.solve().clone()
+    img_off = [int(o) for o in plan.img_off]
+    ksp_off = [int(o) for o in plan.ksp_off]
+    xo = 0
+    for s in range(len(sizes)):
+        p1 = make([sizes[s]], [npts[s]], [coils[s]], trjs[s])
+        p1.set_option(_lib.MRN_OPT_GRID_LANES, 32)  # the batch's lane group (widest slice: 20 coils)
+        p1.set_traj(T(trjs[s].reshape(-1)))
+        n = coils[s] * sizes[s][0] * sizes[s][1]
+        c1 = SenseCG(p1, m_t[img_off[s]:img_off[s] + n], None, 12, 1e-3, 40.0)
+        c1.ksp.copy_(ksp[ksp_off[s]:ksp_off[s] + coils[s] * npts[s]])
+        x1 = c1.solve()
+        nx = sizes[s][0] * sizes[s][1]
+        assert torch.equal(x1, xb[xo:xo + nx]), f"slice {s}"
+        xo += nx
+
+
 def test_sense_cg_graph_matches_oracle():
     from mr_recon_b200.linops import sense_linop
     from mr_recon_b200.recons import CG_SENSE_recon
