@@ -122,8 +122,23 @@ int mrn_sense_normal(mrn_plan* P, const void* x, const void* mps, const float* d
   if (!x || !mps || !out) return MRN_ERR_ARG;
   { StageTimer t(P, kStagePre, ST(s)); RK(launch_pre(P, kPreSense, (const float2*)x, (const float2*)mps, 1.0f, ST(s))); }
   { StageTimer t(P, kStageFft, ST(s)); RK(run_fft(P, CUFFT_FORWARD, ST(s))); }
-  { StageTimer t(P, kStageInterp, ST(s)); RK(launch_interp(P, P->d_grid, kInternal, P->d_ksp_tmp, inv_wd(P), nullptr, ST(s))); }
-  { StageTimer t(P, kStageGrid, ST(s)); RK(launch_grid(P, P->d_ksp_tmp, dcf, kInternal, P->d_grid, inv_wd(P), ST(s))); }
+  if (ent_path_ok(P)) {
+    // 2D: the samples between the two stages in gridding-entry order, with the
+    // density weight applied by the interpolation (the same products, so the
+    // same bits as the sample-order path)
+    const EntIO eio{P->d_ent_of, dcf, P->max_coil, 0};
+    { StageTimer t(P, kStageInterp, ST(s)); RK(launch_interp_reg(P, P->d_grid, kInternal, P->d_ksp_ent, inv_wd(P), nullptr, ST(s), eio)); }
+    {
+      StageTimer t(P, kStageGrid, ST(s));
+      if (P->n_items_grid > 0) {
+        RK(launch_grid_reg(P, P->d_ksp_ent, nullptr, nullptr, kInternal, P->d_grid, inv_wd(P), ST(s), P->max_coil));
+        RK(launch_reduce_split(P, kInternal, P->d_grid, ST(s)));
+      }
+    }
+  } else {
+    { StageTimer t(P, kStageInterp, ST(s)); RK(launch_interp(P, P->d_grid, kInternal, P->d_ksp_tmp, inv_wd(P), nullptr, ST(s))); }
+    { StageTimer t(P, kStageGrid, ST(s)); RK(launch_grid(P, P->d_ksp_tmp, dcf, kInternal, P->d_grid, inv_wd(P), ST(s))); }
+  }
   { StageTimer t(P, kStageFft, ST(s)); RK(run_fft(P, CUFFT_INVERSE, ST(s))); }
   StageTimer t(P, kStagePost, ST(s));
   return launch_post(P, kPostSense, (const float2*)mps, (float2*)out, out_scale, (const float2*)x,

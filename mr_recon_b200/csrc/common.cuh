@@ -73,6 +73,18 @@ __device__ __forceinline__ float2* split_slot(const SplitOut& so, int split, int
   return so.part + (int64_t)(split - 1) * so.slot_stride + (int64_t)coil * so.cell_cap + cell;
 }
 
+// Entry-major samples of a normal operator (2D): between interpolation and
+// gridding the samples live as [gridding entry][stride] (coil c of entry e
+// at e * stride + c), so the interpolation writes one contiguous row of coils
+// per entry of the sample and the gridding reads each batch of entries as
+// one contiguous block instead of gathering one value per coil row.
+struct EntIO {
+  const int* ent_of;  // interpolation: per global point, its gridding entries, [pt][4], -1 past the last
+  const float* dcf;   // interpolation: density weight folded in before the write (or null)
+  int stride;         // > 0: entry-major samples
+  int pad;
+};
+
 constexpr int kKBTerms = 32;  // terms of the I0 power series kept in KBParams
 
 struct KBParams {
@@ -369,6 +381,13 @@ struct mrn_plan {
   size_t cub_tmp_bytes = 0;
   float2* d_grid = nullptr;         // internal oversampled grid (natural order, grouped)
   float2* d_ksp_tmp = nullptr;      // sample scratch for normal operators
+  // 2D normal operator in entry-major sample order (mrn_plan_set_traj): per
+  // point its gridding entries ([M][4] then [M] counters), and the samples
+  // as [entry][max_coil]
+  int* d_ent_of = nullptr;
+  float2* d_ksp_ent = nullptr;
+  int64_t cap_ent_of = 0, cap_ksp_ent = 0;
+  bool ent_ok = false;
   void* toep = nullptr;             // Toeplitz normal operator state (toeplitz.cu), or null
   unsigned* d_sync = nullptr;       // last-block counters: [0] k_cg_dir, [1] CG sums, [2] k_post
   double* d_red = nullptr;          // CG block partial sums, [n_slices][kMaxRedBlocks]

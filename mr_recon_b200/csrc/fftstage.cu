@@ -11,6 +11,8 @@
 // on the way out, for even and odd sizes alike. The oversampled grid is kept
 // in natural FFT order; the interpolation/gridding kernels address centred
 // cell k at storage (k - Nos//2) mod Nos, which is the reference's fftshift.
+#include <algorithm>
+
 #include "common.cuh"
 #include "internal.cuh"
 
@@ -248,12 +250,109 @@ int launch_pre(mrn_plan* P, PreMode mode, const float2* src, const float2* mps, 
   return e == cudaSuccess ? MRN_OK : cuda_fail(e);
 }
 
+// SENSE post with one block per image row and one thread per pixel (the
+// per-warp row kernel above leaves a single 2D image on a few hundred warps):
+// out[q] = scale * apod(q) * sum_c conj(mps_c[q]) Y_c[(q - N//2) mod Nos]
+// (+ lam * xin[q]), coils summed in order as there. With pap the row's
+// Re<xin, out> is a fixed-order block sum into rowpart[row], and the last
+// block adds every slice's rows in row order into pap[slice * pap_stride].
+template <int D>
+__global__ void __launch_bounds__(256)
+k_post_sense(const SliceGeom* __restrict__ sl, int ns, const float* __restrict__ apod,
+             const float2* __restrict__ grid, const float2* __restrict__ mps, float scale,
+             float2* __restrict__ out, const float2* __restrict__ xin, float lam,
+             double* __restrict__ pap, int pap_stride, double* __restrict__ rowpart,
+             unsigned* __restrict__ counter) {
+  __shared__ double red[8];
+  const int64_t row = blockIdx.x;
+  const int s = slice_by_row(sl, ns, row, 2);
+  const SliceGeom& g = sl[s];
+  int64_t o = row - g.xrow_off;
+  const int64_t orow = o;
+  float aout = scale * g.inv_sqrt_n;
+  int64_t slin = 0;
+  int q[kMaxDim] = {0, 0, 0};
+  for (int i = D - 2; i >= 0; --i) {
+    q[i] = (int)(o % g.n[i]);
+    o /= g.n[i];
+  }
+  for (int i = 0; i < D - 1; ++i) {
+    aout *= apod[g.apod_off[i] + q[i]];
+    int sidx = q[i] - g.n[i] / 2;
+    if (sidx < 0) sidx += g.nos[i];
+    slin = slin * g.nos[i] + sidx;
+  }
+  const int nl = g.n[D - 1], nosl = g.nos[D - 1], h = nl / 2;
+  slin *= nosl;
+  const float* al = apod + g.apod_off[D - 1];
+  const float2* gbase = grid + g.grid_off + slin;
+  const float2* mbase = mps + g.img_off + orow * nl;
+  float2* orow_p = out + g.x_off + orow * nl;
+  const float2* xrow = xin ? xin + g.x_off + orow * nl : nullptr;
+  double part = 0.0;
+  for (int j = threadIdx.x; j < nl; j += blockDim.x) {
+    int sj = j - h;
+    if (sj < 0) sj += nosl;
+    float ax = 0.f, ay = 0.f;
+#pragma unroll 8
+    for (int c = 0; c < g.ncoil; ++c) {
+      const float2 y = gbase[(int64_t)c * g.gos + sj];
+      const float2 m = __ldg(mbase + (int64_t)c * g.nimg + j);
+      // conj(m) * y
+      ax += m.x * y.x + m.y * y.y;
+      ay += m.x * y.y - m.y * y.x;
+    }
+    const float a = aout * al[j];
+    float2 v = make_float2(ax * a, ay * a);
+    if (xrow) {
+      const float2 xv = xrow[j];
+      v.x += lam * xv.x;
+      v.y += lam * xv.y;
+      part += (double)xv.x * v.x + (double)xv.y * v.y;
+    }
+    orow_p[j] = v;
+  }
+  if (!pap) return;
+  for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) red[warp] = part;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    rowpart[row] = t;
+  }
+  __syncthreads();  // the row partial is stored before thread 0 arrives
+  if (!arrive_last_block(counter, gridDim.x)) return;
+  for (int qs = warp; qs < ns; qs += (int)(blockDim.x >> 5)) {
+    const SliceGeom& gq = sl[qs];
+    const double v = warp_sum_fixed(rowpart + gq.xrow_off, gq.nimg / gq.n[D - 1], lane);
+    if (lane == 0) pap[(int64_t)qs * pap_stride] += v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *counter = 0u;
+}
+
 int launch_post(mrn_plan* P, PostMode mode, const float2* mps, float2* out, float scale,
                 const float2* xin, float lam, double* pap, int pap_stride, cudaStream_t st) {
   const int64_t nrows = mode == kPostSense ? P->n_xrow : P->n_irow;
   if (mode != kPostSense) pap = nullptr;  // Re<x, out> exists only for the SENSE form
   const unsigned blocks = (unsigned)((nrows + 7) / 8);
   if (blocks == 0) return MRN_OK;
+  if (mode == kPostSense) {
+    int nl = 1;
+    for (const auto& g : P->h_slices) nl = std::max(nl, g.n[P->ndim - 1]);
+    const unsigned threads = nl <= 64 ? 64 : (nl <= 128 ? 128 : 256);
+    const unsigned rows = (unsigned)nrows;
+    if (P->ndim == 1)
+      k_post_sense<1><<<rows, threads, 0, st>>>(P->d_slices, P->nslices, P->d_apod, P->d_grid, mps, scale, out, xin, lam, pap, pap_stride, P->d_rowpart, P->d_sync + 2);
+    else if (P->ndim == 2)
+      k_post_sense<2><<<rows, threads, 0, st>>>(P->d_slices, P->nslices, P->d_apod, P->d_grid, mps, scale, out, xin, lam, pap, pap_stride, P->d_rowpart, P->d_sync + 2);
+    else
+      k_post_sense<3><<<rows, threads, 0, st>>>(P->d_slices, P->nslices, P->d_apod, P->d_grid, mps, scale, out, xin, lam, pap, pap_stride, P->d_rowpart, P->d_sync + 2);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? MRN_OK : cuda_fail(e);
+  }
   if (P->ndim == 1)
     k_post<1><<<blocks, 256, 0, st>>>(P->d_slices, P->nslices, P->d_apod, P->d_grid, mps, mode, scale, out, xin, lam, pap, pap_stride, nrows, P->d_rowpart, P->d_sync + 2);
   else if (P->ndim == 2)

@@ -57,7 +57,7 @@ int launch_grid_warp(mrn_plan* P, const float2* ksp, const float* dcf, const flo
                      int layout, float2* grid, float scale, cudaStream_t st);
 bool interp_reg_ok(const mrn_plan* P);
 int launch_interp_reg(mrn_plan* P, const float2* grid, int layout, float2* ksp, float scale,
-                      const float2* temporal, cudaStream_t st);
+                      const float2* temporal, cudaStream_t st, EntIO eio = EntIO{nullptr, nullptr, 0, 0});
 int launch_trajgrad_reg(mrn_plan* P, const float2* grid, int layout, const float2* samples, float* out,
                         float scale, cudaStream_t st);
 bool grid_reg_ok(const mrn_plan* P);
@@ -65,7 +65,11 @@ bool grid_reg3_ok(const mrn_plan* P);
 int launch_grid_reg3(mrn_plan* P, const float2* ksp, const float* dcf, const float2* temporal,
                      int layout, float2* grid, float scale, cudaStream_t st);
 int launch_grid_reg(mrn_plan* P, const float2* ksp, const float* dcf, const float2* temporal,
-                    int layout, float2* grid, float scale, cudaStream_t st);
+                    int layout, float2* grid, float scale, cudaStream_t st, int ent_stride = 0);
+// 2D normal operator with entry-major samples (EntIO): the entry map is bound
+// and the register interpolation and gridding kernels apply
+bool ent_path_ok(const mrn_plan* P);
+int launch_reduce_split(mrn_plan* P, GridLayout layout, float2* grid, cudaStream_t st);
 // 2D weight tables (wtab.cu)
 bool wtab_applicable(const mrn_plan* P);
 int build_wtabs(mrn_plan* P, cudaStream_t st);

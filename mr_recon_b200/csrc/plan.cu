@@ -157,6 +157,17 @@ __global__ void k_emit_entries(const SliceGeom* __restrict__ sl, int ns, int ndi
       }
 }
 
+// Per point, the gridding entries it was emitted as (positions after the
+// tile sort); the slot order among a point's entries does not matter.
+__global__ void k_point_entries(const int* __restrict__ perm_g, int64_t ne, int* __restrict__ ent_of,
+                                int* __restrict__ cnt) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  const int p = perm_g[e];
+  const int k = atomicAdd(cnt + p, 1);
+  if (k < 4) ent_of[(int64_t)p * 4 + k] = (int)e;
+}
+
 __global__ void k_gather_coords(const float4* __restrict__ src, const int* __restrict__ perm,
                                 int64_t n, float4* __restrict__ dst) {
   int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -763,7 +774,8 @@ int mrn_plan_destroy(mrn_plan* P) {
                   P->d_items_g, P->d_counts, P->d_split_tiles, P->d_cub_tmp, P->d_grid,
                   P->d_ksp_tmp, P->d_sync, P->d_wmeta_i, P->d_wtab_i, P->d_wmeta_g,
                   P->d_wtab_g, P->d_part, P->d_items_tmp, P->d_sort_key[0], P->d_sort_key[1],
-                  P->d_sort_idx[0], P->d_sort_idx[1], P->d_red, P->d_rowpart};
+                  P->d_sort_idx[0], P->d_sort_idx[1], P->d_red, P->d_rowpart, P->d_ent_of,
+                  P->d_ksp_ent};
   for (void* b : bufs)
     if (b) cudaFree(b);
   delete P;
@@ -964,6 +976,24 @@ int mrn_plan_set_traj(mrn_plan* P, const float* trj, void* stream_) {
   RK(make_items(T, chunk, 0, max_items_i, 0, 0, P->d_tile_start_i, P->d_tile_end_i, P->d_items_i));
   RK(make_items(TG, gchunk, 1, max_items_g, 1, 1, P->d_tile_start_g, P->d_tile_end_g, P->d_items_g));
   RK(build_wtabs(P, st));
+  // 2D (at most 4 entries per point): the entry map of the entry-major normal operator
+  P->ent_ok = false;
+  if (ndim == 2 && !(P->flags & MRN_PLAN_RAW) && M > 0 && E > 0) {
+    if (P->cap_ent_of < 5 * M) {
+      RK(dev_alloc(&P->d_ent_of, (size_t)(5 * M)));
+      P->cap_ent_of = 5 * M;
+    }
+    const int64_t ke = E * (int64_t)P->max_coil;
+    if (P->cap_ksp_ent < ke) {
+      RK(dev_alloc(&P->d_ksp_ent, (size_t)ke));
+      P->cap_ksp_ent = ke;
+    }
+    CK(cudaMemsetAsync(P->d_ent_of, 0xff, (size_t)(4 * M) * sizeof(int), st));
+    CK(cudaMemsetAsync(P->d_ent_of + 4 * M, 0, (size_t)M * sizeof(int), st));
+    k_point_entries<<<blocks_for(E), 256, 0, st>>>(P->d_perm_g, E, P->d_ent_of, P->d_ent_of + 4 * M);
+    CK(cudaGetLastError());
+    P->ent_ok = true;
+  }
   P->n_items_interp = max_items_i;
   P->n_items_grid = max_items_g;
   P->n_split = max_split;

@@ -797,7 +797,7 @@ int launch_grid(mrn_plan* P, const float2* ksp, const float* dcf, GridLayout lay
   return launch_grid_t(P, ksp, dcf, nullptr, layout, grid, scale, st);
 }
 
-static int launch_reduce_split(mrn_plan* P, GridLayout layout, float2* grid, cudaStream_t st) {
+int launch_reduce_split(mrn_plan* P, GridLayout layout, float2* grid, cudaStream_t st) {
   if (P->n_split == 0) return MRN_OK;
   const int groups = (P->max_coil + kSplitCoils - 1) / kSplitCoils;
   const int64_t units = P->n_split * groups;

@@ -623,7 +623,7 @@ __global__ void __launch_bounds__(kRegInterpWarps * 32, (D == 3 && K > 5) ? 2 : 
 k_interp_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBParams kb,
              const float4* __restrict__ coord, const int* __restrict__ perm,
              const float2* __restrict__ grid, int layout, float2* __restrict__ ksp, float scale,
-             const float2* __restrict__ temporal, int cg) {
+             const float2* __restrict__ temporal, int cg, EntIO eio) {
   constexpr int CW = 32 / SUB, CS = CW + 1, NW = kRegInterpWarps, NT = NW * 32;
   extern __shared__ float4 smem_f4[];
   float2* region = reinterpret_cast<float2*>(smem_f4);
@@ -695,6 +695,20 @@ k_interp_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, K
         h = make_float2(scale * t.x, scale * t.y);
       }
       const float2 v = make_float2(acc.x * h.x - acc.y * h.y, acc.x * h.y + acc.y * h.x);
+      if (eio.stride > 0) {  // entry-major: one contiguous row of coils per entry of the sample
+        const int64_t pg = pt_off + lp;
+        float2 vv = v;
+        if (eio.dcf) {
+          const float d = eio.dcf[pg];
+          vv = make_float2(v.x * d, v.y * d);
+        }
+        const int4 es = *reinterpret_cast<const int4*>(eio.ent_of + pg * 4);
+        const int ee[4] = {es.x, es.y, es.z, es.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (ee[q] >= 0) ksp[(int64_t)ee[q] * eio.stride + c0 + coil] = vv;
+        continue;
+      }
       float2* dst = kspc + lp;
       if (temporal) {
         const float2 o = *dst;
@@ -939,7 +953,7 @@ k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBP
            const float4* __restrict__ coord, const int* __restrict__ perm,
            const float2* __restrict__ ksp, const float* __restrict__ dcf,
            const float2* __restrict__ temporal, float2* __restrict__ grid, int layout, float scale,
-           int cg, SplitOut so) {
+           int cg, SplitOut so, int ent_stride) {
   constexpr int T = kRegTile, R = kRegRows, B = kRegBatch, CW = 32 / SUB;
   __shared__ G2Smem<CW> sm;
   auto& s_c = sm.b.c;
@@ -977,8 +991,14 @@ k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBP
   // values (per entry and coil), densities and temporal weights of batch bi
   auto copy_values = [&](int bi) {
     const int nb = batch_len(bi), b2 = bi & 1, r3 = bi % 3;
-    if (has_coil)
-      for (int j = sid; j < nb; j += 2 * SUB) cp_async8(&s_v[b2][j][coil], kspc + (s_pm[r3][j] - pt_off));
+    if (has_coil) {
+      if (ent_stride > 0) {  // entry-major samples: the batch's rows are contiguous
+        const float2* eb = ksp + (int64_t)(it.start + bi * B) * ent_stride + c0 + coil;
+        for (int j = sid; j < nb; j += 2 * SUB) cp_async8(&s_v[b2][j][coil], eb + (int64_t)j * ent_stride);
+      } else {
+        for (int j = sid; j < nb; j += 2 * SUB) cp_async8(&s_v[b2][j][coil], kspc + (s_pm[r3][j] - pt_off));
+      }
+    }
     if (tid < nb) {
       if (dcf) cp_async4(&s_d[b2][tid], dcf + s_pm[r3][tid]);
     } else if (tid >= 32 && tid - 32 < nb) {
@@ -1234,7 +1254,7 @@ bool interp_reg_ok(const mrn_plan* P) {
 }
 
 int launch_interp_reg(mrn_plan* P, const float2* grid, int layout, float2* ksp, float scale,
-                      const float2* temporal, cudaStream_t st) {
+                      const float2* temporal, cudaStream_t st, EntIO eio) {
   if (P->n_items_interp == 0) return MRN_OK;
   int cg, ng;
   const int sub = interp_reg_sub(P, &cg, &ng);
@@ -1248,7 +1268,8 @@ int launch_interp_reg(mrn_plan* P, const float2* grid, int layout, float2* ksp, 
     rc = prep_attr(kern, smem);                                                                     \
     if (rc == MRN_OK)                                                                               \
       kern<<<gdim, kRegInterpWarps * 32, smem, st>>>(P->d_items_i, P->d_slices, P->kb, P->d_coord_i, \
-                                                     P->d_perm_i, grid, layout, ksp, scale, temporal, cg); \
+                                                     P->d_perm_i, grid, layout, ksp, scale, temporal, cg, \
+                                                     eio);                                            \
   } while (0)
 #define MRN_IREG_SUB(DD, KK)                     \
   if (sub == 4) MRN_IREG_LAUNCH(DD, KK, 4);      \
@@ -1305,12 +1326,17 @@ int launch_trajgrad_reg(mrn_plan* P, const float2* grid, int layout, const float
   return e == cudaSuccess ? MRN_OK : cuda_fail(e);
 }
 
+bool ent_path_ok(const mrn_plan* P) {
+  return P->ent_ok && P->ndim == 2 && P->use_fast && fast_path_ok(P, false) && interp_reg_ok(P) &&
+         fast_path_ok(P, true) && P->warp_grid && grid_reg_ok(P) && P->cap_ksp_ent >= P->n_entries_grid * P->max_coil;
+}
+
 bool grid_reg_ok(const mrn_plan* P) {
   return P->reg_grid && P->ndim == 2 && P->tmax_gcells[0] <= kRegTile && P->tmax_gcells[1] <= kRegTile;
 }
 
 int launch_grid_reg(mrn_plan* P, const float2* ksp, const float* dcf, const float2* temporal,
-                    int layout, float2* grid, float scale, cudaStream_t st) {
+                    int layout, float2* grid, float scale, cudaStream_t st, int ent_stride) {
   if (P->n_items_grid == 0) return MRN_OK;
   int cg = P->coil_group_req > 0 ? std::min(P->coil_group_req, P->max_coil) : P->max_coil;
   cg = std::max(1, std::min(cg, 32));
@@ -1325,7 +1351,7 @@ int launch_grid_reg(mrn_plan* P, const float2* ksp, const float* dcf, const floa
 #define MRN_REG_LAUNCH(KK, SS)                                                              \
   k_grid_reg<KK, SS><<<gdim, 64, 0, st>>>(P->d_items_g, P->d_slices, P->kb, P->d_coord_g, \
                                           P->d_perm_g, ksp, dcf, temporal, grid, layout, scale, cg, \
-                                          split_out(P))
+                                          split_out(P), ent_stride)
 #define MRN_REG_SUB(KK)                     \
   if (sub == 4) MRN_REG_LAUNCH(KK, 4);      \
   else if (sub == 2) MRN_REG_LAUNCH(KK, 2); \

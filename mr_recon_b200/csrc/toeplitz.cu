@@ -252,6 +252,77 @@ k_toep_post(const ToepGeom* __restrict__ tg, int ns, const float2* __restrict__ 
   if (threadIdx.x == 0) *counter = 0u;
 }
 
+// SENSE form of the post step with one block per image row and one thread
+// per pixel (same per-pixel arithmetic and coil order as k_toep_post; the
+// row's Re<xin, out> is a fixed-order block sum).
+template <int D>
+__global__ void __launch_bounds__(256)
+k_toep_post_sense(const ToepGeom* __restrict__ tg, int ns, const float2* __restrict__ grid,
+                  const float2* __restrict__ mps, float scale, float2* __restrict__ out,
+                  const float2* __restrict__ xin, float lam, double* __restrict__ pap, int pap_stride,
+                  double* __restrict__ rowpart, unsigned* __restrict__ counter) {
+  __shared__ double red[8];
+  const int64_t row = blockIdx.x;
+  const ToepGeom& g = tg[toep_slice(tg, ns, row, 2)];
+  int64_t o = row - g.xrow_off;
+  const int64_t orow = o;
+  int q[kMaxDim] = {0, 0, 0};
+  for (int i = D - 2; i >= 0; --i) {
+    q[i] = (int)(o % g.n[i]);
+    o /= g.n[i];
+  }
+  int64_t slin = 0;
+  for (int i = 0; i < D - 1; ++i) {
+    int sidx = q[i] + g.off[i] - g.np[i] / 2;
+    if (sidx < 0) sidx += g.np[i];
+    slin = slin * g.np[i] + sidx;
+  }
+  const int nl = g.n[D - 1], npl = g.np[D - 1], sh = g.off[D - 1] - npl / 2;
+  slin *= npl;
+  float2* orow_p = out + g.x_off + orow * nl;
+  const float2* xrow = xin ? xin + g.x_off + orow * nl : nullptr;
+  double part = 0.0;
+  for (int j = threadIdx.x; j < nl; j += blockDim.x) {
+    int sj = j + sh;
+    if (sj < 0) sj += npl;
+    float ax = 0.f, ay = 0.f;
+#pragma unroll 8
+    for (int c = 0; c < g.ncoil; ++c) {
+      const float2 y = grid[g.grid_off + (int64_t)c * g.gp + slin + sj];
+      const float2 m = __ldg(mps + g.img_off + (int64_t)c * g.nimg + orow * nl + j);
+      ax += m.x * y.x + m.y * y.y;  // conj(m) * y
+      ay += m.x * y.y - m.y * y.x;
+    }
+    float2 v = make_float2(ax * scale, ay * scale);
+    if (xrow) {
+      const float2 xv = xrow[j];
+      v.x += lam * xv.x;
+      v.y += lam * xv.y;
+      part += (double)xv.x * v.x + (double)xv.y * v.y;
+    }
+    orow_p[j] = v;
+  }
+  if (!pap) return;
+  for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) red[warp] = part;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    rowpart[row] = t;
+  }
+  __syncthreads();
+  if (!arrive_last_block(counter, gridDim.x)) return;
+  for (int qs = warp; qs < ns; qs += (int)(blockDim.x >> 5)) {
+    const ToepGeom& gq = tg[qs];
+    const double v = warp_sum_fixed(rowpart + gq.xrow_off, gq.nimg / gq.n[D - 1], lane);
+    if (lane == 0) pap[(int64_t)qs * pap_stride] += v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *counter = 0u;
+}
+
 static ToepState* toep(mrn_plan* P) { return static_cast<ToepState*>(P->toep); }
 
 void toep_free(mrn_plan* P) {
@@ -416,6 +487,20 @@ static int toep_apply(mrn_plan* P, const float2* src, const float2* mps, float2*
   const int64_t nrows = mps ? P->n_xrow : P->n_irow;
   const unsigned nb = (unsigned)((nrows + 7) / 8);
   if (nb == 0) return MRN_OK;
+  if (mps) {
+    int nl = 1;
+    for (const auto& tgh : T->h) nl = std::max(nl, tgh.n[D - 1]);
+    const unsigned threads = nl <= 64 ? 64 : (nl <= 128 ? 128 : 256);
+    const unsigned rows = (unsigned)nrows;
+    if (D == 1)
+      k_toep_post_sense<1><<<rows, threads, 0, st>>>(T->d, ns, T->grid, mps, scale, out, xin, lam, pap, pap_stride, P->d_rowpart, P->d_sync + 3);
+    else if (D == 2)
+      k_toep_post_sense<2><<<rows, threads, 0, st>>>(T->d, ns, T->grid, mps, scale, out, xin, lam, pap, pap_stride, P->d_rowpart, P->d_sync + 3);
+    else
+      k_toep_post_sense<3><<<rows, threads, 0, st>>>(T->d, ns, T->grid, mps, scale, out, xin, lam, pap, pap_stride, P->d_rowpart, P->d_sync + 3);
+    CKT(cudaGetLastError());
+    return MRN_OK;
+  }
   if (!mps) pap = nullptr;
   if (D == 1)
     k_toep_post<1><<<nb, 256, 0, st>>>(T->d, ns, T->grid, mps, scale, out, xin, lam, pap, pap_stride, nrows, P->d_rowpart, P->d_sync + 3);
