@@ -490,7 +490,7 @@ def test_uneven_batched_cg_equals_per_slice_solves_bitwise():
         xo += nx
 
 
-@pytest.mark.parametrize("coils", [32, 12, 5])
+@pytest.mark.parametrize("coils", [40, 32, 12, 5])
 def test_sense_normal_entry_major_equals_forward_then_adjoint(coils):
     """The 2D SENSE normal operator keeps its samples in gridding-entry order
     (the density weight applied by the interpolation): it must give exactly
