@@ -126,6 +126,13 @@ int mrn_plan_stats(mrn_plan* plan, int64_t* out4);
  * one-slice plan given the lane count of a larger uneven plan (the lanes its
  * widest slice needs) adds every cell in the same order as that plan. */
 #define MRN_OPT_GRID_LANES 10
+/* MRN_OPT_ENTRY_MAJOR (default 1): in 2D, mrn_plan_set_traj also builds the
+ * map from samples to gridding entries and a sample buffer of 8 * (largest
+ * coil count) bytes per gridding entry (about 2.7x the k-space at width 6),
+ * so that mrn_sense_normal keeps its samples in entry order between the
+ * interpolation and the gridding (contiguous rows instead of per-coil
+ * gathers; the same bits). 0 skips both; set before mrn_plan_set_traj. */
+#define MRN_OPT_ENTRY_MAJOR 11
 int mrn_plan_set_option(mrn_plan* plan, int option, int value);
 
 /* Kaiser-Bessel beta per dimension for a raw (MRN_PLAN_RAW) plan, beta[0..ndim),

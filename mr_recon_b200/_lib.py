@@ -37,6 +37,7 @@ MRN_OPT_GRID_TILE = 7
 MRN_OPT_REG_GRIDDING = 8
 MRN_OPT_REG_INTERP = 9
 MRN_OPT_GRID_LANES = 10
+MRN_OPT_ENTRY_MAJOR = 11
 
 _vp = C.c_void_p
 _i = C.c_int

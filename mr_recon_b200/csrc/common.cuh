@@ -388,6 +388,7 @@ struct mrn_plan {
   float2* d_ksp_ent = nullptr;
   int64_t cap_ent_of = 0, cap_ksp_ent = 0;
   bool ent_ok = false;
+  bool use_ent = true;   // option: build the entry map at mrn_plan_set_traj
   void* toep = nullptr;             // Toeplitz normal operator state (toeplitz.cu), or null
   unsigned* d_sync = nullptr;       // last-block counters: [0] k_cg_dir, [1] CG sums, [2] k_post
   double* d_red = nullptr;          // CG block partial sums, [n_slices][kMaxRedBlocks]

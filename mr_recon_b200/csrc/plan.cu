@@ -716,6 +716,10 @@ int mrn_plan_set_option(mrn_plan* P, int option, int value) {
     case MRN_OPT_WEIGHT_TABLES: P->use_wtab = value != 0; return MRN_OK;
     case MRN_OPT_REG_GRIDDING: P->reg_grid = value != 0; return MRN_OK;
     case MRN_OPT_REG_INTERP: P->reg_interp = value != 0; return MRN_OK;
+    case MRN_OPT_ENTRY_MAJOR:
+      P->use_ent = value != 0;
+      P->traj_set = false;  // the entry map is built (or not) at mrn_plan_set_traj
+      return MRN_OK;
     case MRN_OPT_GRID_LANES:
       if (value != 0 && value != 8 && value != 16 && value != 32) return MRN_ERR_ARG;
       P->grid_lanes = value;
@@ -978,7 +982,7 @@ int mrn_plan_set_traj(mrn_plan* P, const float* trj, void* stream_) {
   RK(build_wtabs(P, st));
   // 2D (at most 4 entries per point): the entry map of the entry-major normal operator
   P->ent_ok = false;
-  if (ndim == 2 && !(P->flags & MRN_PLAN_RAW) && M > 0 && E > 0) {
+  if (P->use_ent && ndim == 2 && !(P->flags & MRN_PLAN_RAW) && M > 0 && E > 0) {
     if (P->cap_ent_of < 5 * M) {
       RK(dev_alloc(&P->d_ent_of, (size_t)(5 * M)));
       P->cap_ent_of = 5 * M;

@@ -234,6 +234,8 @@ class _LowRankPlan:
                          max_chunk=nufft.max_chunk, device=dev, fast=nufft.fast,
                          warp_grid=nufft.warp_grid, weight_tables=nufft.weight_tables,
                          reg_grid=nufft.reg_grid, reg_interp=nufft.reg_interp)
+        # the low-rank calls never run the SENSE normal's entry-order samples
+        self.plan.set_option(_lib.MRN_OPT_ENTRY_MAJOR, 0)
         self.plan.set_traj(trj.reshape(1, M, d).expand(J, M, d).contiguous().reshape(-1))
         self.mps = mps.to(complex_dtype).reshape(1, -1).expand(J, -1).contiguous().reshape(-1)
         self.w_fwd = weights.to(complex_dtype).reshape(J, M).contiguous()

@@ -599,6 +599,40 @@ class SubspaceOracle:
                          for k in range(self.phi.shape[0])]).astype(C64)
 
 
+def subspace_toeplitz_normal(trj, mps, phi, alphas, nufft: KBNufftOracle, dcf=None, os_factor=2.0):
+    """Toeplitz normal of subspace_linop: kernels K[k1][k2] of the weights
+    conj(phi_k1(t)) phi_k2(t) dcf(t) (linops.py:1581-1601, phi along the last
+    trajectory dimension) and out[i] = sum_c conj(S_c) crop(IFFT(sum_k
+    K[i][k] FFT(pad(S_c alpha_k)))) with orthonormal centred FFTs
+    (linops.py:1703-1772)."""
+    trj = np.asarray(trj, dtype=F32)
+    tshape = trj.shape[:-1]
+    d = nufft.d
+    phi = np.asarray(phi).astype(C64)
+    K = phi.shape[0]
+    ph = phi.reshape((K,) + (1,) * (len(tshape) - 1) + (tshape[-1],))
+    dcf = np.ones(tshape, F32) if dcf is None else np.asarray(dcf, F32)
+    kern = None
+    for k1 in range(K):
+        for k2 in range(K):
+            w = np.broadcast_to(np.conj(ph[k1]) * ph[k2] * dcf, tshape).astype(C64)
+            kk = nufft.calc_toeplitz_kernels(trj[None], w[None], os_factor)[0]
+            if kern is None:
+                kern = np.zeros((K, K) + kk.shape, dtype=C64)
+            kern[k1, k2] = kk
+    im_os = kern.shape[2:]
+    mps = np.asarray(mps).astype(C64)
+    axes = tuple(range(-d, 0))
+    sx = mps[:, None] * np.asarray(alphas).astype(C64)[None]  # C K *im
+    fx = fft_c(resize(sx, sx.shape[:2] + tuple(im_os)), axes=axes, norm="ortho")
+    out = np.zeros_like(np.asarray(alphas), dtype=C64)
+    for i in range(K):
+        mf = np.einsum("k...,ck...->c...", kern[i], fx)
+        y = resize(ifft_c(mf, axes=axes, norm="ortho"), mps.shape)
+        out[i] = (y * np.conj(mps)).sum(0)
+    return out.astype(C64)
+
+
 def _vdot_real(a, b):
     return float(np.real(np.vdot(a.astype(np.complex128), b.astype(np.complex128))))
 

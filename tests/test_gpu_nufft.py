@@ -507,9 +507,35 @@ def test_sense_normal_entry_major_equals_forward_then_adjoint(coils):
     x = T(synth.randn_complex(im, rng))
     n = A.normal(x)
     assert torch.equal(n, A.adjoint(A.forward(x)))
+    # the same plan without the entry map runs the sample-order normal: same bits
+    from mr_recon_b200 import _lib
+    A.plan.set_option(_lib.MRN_OPT_ENTRY_MAJOR, 0)
+    A.plan.set_traj(A.trj.contiguous())
+    assert torch.equal(A.normal(x), n)
     on = O.KBNufftOracle(im, 1.25, 6)
     Ao = O.SenseOracle(trj, mps, on, dcf=dcf)
     assert rel(Nn(n), Ao.normal(Nn(x))) < TOL
+
+
+def test_subspace_linop_toeplitz_normal_matches_oracle():
+    """subspace_linop(use_toeplitz=True): the nsub x nsub kernels of the
+    weights conj(phi_k1) phi_k2 dcf on the B200 adjoint and the FFT-only
+    normal (linops.py:1581-1601, 1703-1772) against the oracle's restatement;
+    close to the exact normal A^H A (the Toeplitz model error)."""
+    from mr_recon_b200.linops import subspace_linop
+    rng = np.random.RandomState(61)
+    im, C, K = (24, 20), 3, 2
+    trj = synth.vd_spiral(4, 240, 10.0).transpose(1, 0, 2).copy()  # (nro 240, ntr 4, 2)
+    phi = synth.randn_complex((K, 4), rng)
+    mps = synth.gaussian_coil_maps(im, C).astype(np.complex64)
+    dcf = (0.5 + rng.rand(240, 4)).astype(np.float32)
+    A = subspace_linop(im, T(trj), T(mps), T(phi), dcf=T(dcf), nufft=b200_nufft(im), use_toeplitz=True)
+    a = synth.randn_complex((K, *im), rng)
+    ref = O.subspace_toeplitz_normal(trj, mps, phi, a, O.KBNufftOracle(im, 1.25, 6), dcf=dcf)
+    out = Nn(A.normal(T(a)))
+    assert rel(out, ref) < 1e-4
+    Ao = O.SubspaceOracle(trj, mps, phi, O.KBNufftOracle(im, 1.25, 6), dcf=dcf)
+    assert rel(out, Ao.adjoint(Ao.forward(a))) < 5e-2
 
 
 def test_sense_cg_graph_matches_oracle():
