@@ -28,27 +28,30 @@ namespace mrn {
 // Footprint windows. With K candidate taps per dimension a sample's footprint
 // has K - 1 = KW taps per dimension unless u - W/2 is an integer (then the
 // K-th candidate lies exactly on the support boundary and carries weight), so
-// in y and z the part of a footprint inside the tile fits a window of KW
-// cells starting at w0 in [0, NW), NW = 8 - KW + 1 (clamped to the tile; a
-// footprint that is cut by the tile edge has zero weights in the window's
-// outside cells). The window start pair (y0, z0) is the same for every
-// thread of the CTA (they all accumulate the same entry), so one warp-uniform
-// binary dispatch over the NW^2 pairs selects a straight-line block of KW
+// in every dimension the part of a footprint inside the tile fits a window of
+// KW cells starting at w0 in [0, NW), NW = 8 - KW + 1 (clamped to the tile; a
+// footprint cut by the tile edge has zero weights in the window's outside
+// cells). Each window weight is evaluated directly from its tap (no
+// tile-aligned vector is built). The window start pair (y0, z0) is the same
+// for every thread of the CTA (they all accumulate the same entry), so one
+// warp-uniform binary dispatch over the NW^2 pairs selects a straight-line block of KW
 // rows x KW cells of packed two-lane FMAs (fma.rn.f32x2: re and im of a
 // cell) on fixed registers: no FMA touches a cell outside the window and no
-// row needs a test. Entries with K taps inside the tile in y or z (exact
-// boundary taps) take the dense block: tile-aligned weights, warp-uniform
-// skips of rows without weight, 8 cells per row.
+// row needs a test. A thread takes the x weight of its plane from the x
+// window. Entries with K taps inside the tile in some dimension (exact
+// boundary taps, a handful per spoke through the k-space centre) take the
+// dense block instead: the warp evaluates the tile-aligned weights of all
+// three dimensions itself (one lane per cell) and skips rows without weight.
 //
-// The weights (x tile-aligned and carrying the scale; y and z both as windows
-// and tile-aligned) and the sample values reach shared memory in batches of
-// 64 entries through a cp.async pipeline: in iteration b the values of batch
+// The weights and the sample values reach shared memory in batches of 64
+// entries through a cp.async pipeline: in iteration b the values of batch
 // b+1 and the coordinates of batch b+3 are in flight while the weights of
 // batch b+1 are evaluated and batch b is accumulated; one barrier per batch.
-// Each warp takes one ballot per 32 entries of those with weight on its two
-// planes. No atomics; float32 accumulation in entry order, so results are the
-// same on every run (split tiles write partial tiles that a reduction pass
-// adds in item order).
+// Each entry carries the mask of its x-planes with weight, so a warp takes
+// one ballot per 32 entries of those touching its two planes without a
+// weight load. No atomics; float32 accumulation in entry order, so results
+// are the same on every run (split tiles write partial tiles that a
+// reduction pass adds in item order).
 // ---------------------------------------------------------------------------
 constexpr int kG3Tile = 8;
 constexpr int kG3Batch = 64;
@@ -59,18 +62,18 @@ namespace {
 
 template <int B>
 struct G3Smem {
-  float4 c[3][B];        // coordinate ring
-  int pm[3][B];          // sample index ring
-  float wx[2][B][8];     // per entry: tile-aligned x weights x scale
-  float wyt[2][B][8];    // per entry: tile-aligned y weights (dense block)
-  float wzt[2][B][8];    // per entry: tile-aligned z weights (dense block)
-  float wyw[2][B][8];    // per entry: y weights of the window (first KW used)
-  float2 wzw[2][B][8];   // per entry: z weights of the window, each twice
-  int2 code[2][B];       // per entry: window starts (y0, z0); NW = dense
-  float2 v[2][B][kG3Coils];  // per entry and coil: sample value
+  float4 c[4][B];        // coordinate ring (a batch stays until it is accumulated)
+  int pm[4][B];          // sample index ring
+  float wxw[2][B][8];    // per entry: x window weights x scale (first KW used)
+  float wyw[2][B][8];    // per entry: y window weights
+  float2 wzw[2][B][8];   // per entry: z window weights, each twice
+  unsigned code[2][B];   // per entry: bytes x0, y0, z0 (bit 3: dense), x-plane mask
+  float2 v[2][B][kG3Coils + 1];  // per entry and coil: sample value (row padded: conflict-free copies)
   float d[2][B];         // per entry: density weight
   float2 t[2][B];        // per entry: temporal weight
 };
+
+constexpr unsigned kG3Dense = 0x080808u;
 
 // KW rows x KW cells of the window at (Y0, Z0): acc[Y0 + r][Z0 + c] +=
 // wy[r] wz[c] v for the thread's coil and plane (v already carries the x
@@ -133,31 +136,43 @@ k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
   const int nbatch = (it.count + B - 1) / B;
   auto batch_len = [&](int bi) { return bi < nbatch ? min(B, it.count - bi * B) : 0; };
 
-  // coordinates and sample indices of batch bi into ring slot bi % 3
+  // coordinates and sample indices of batch bi into ring slot bi % 4
   auto copy_coords = [&](int bi) {
-    const int nb = batch_len(bi), r3 = bi % 3;
-    if (tid < nb) cp_async16(&s.c[r3][tid], coord + it.start + bi * B + tid);
-    else if (tid >= B && tid - B < nb) cp_async4(&s.pm[r3][tid - B], perm + it.start + bi * B + tid - B);
+    const int nb = batch_len(bi), r4 = bi & 3;
+    if (tid < nb) cp_async16(&s.c[r4][tid], coord + it.start + bi * B + tid);
+    else if (tid >= B && tid - B < nb) cp_async4(&s.pm[r4][tid - B], perm + it.start + bi * B + tid - B);
   };
-  // sample values (one 8-byte copy per entry and coil), densities, temporal weights
+  // sample values (one 8-byte copy per entry and coil), densities, temporal
+  // weights; thread = (entry tid % B, coil phase tid / B), so one warp copy
+  // reads 32 entries of one coil row (consecutive samples share lines)
   auto copy_values = [&](int bi) {
-    const int nb = batch_len(bi), b2 = bi & 1, r3 = bi % 3;
-    for (int k = tid; k < B * CW; k += NT) {
-      const int j = k >> 4, c = k & 15;
-      if (j < nb && c < ncg) cp_async8(&s.v[b2][j][c], kspg + (int64_t)c * m + (s.pm[r3][j] - pt_off));
+    const int nb = batch_len(bi), b2 = bi & 1, r4 = bi & 3;
+    const int j = tid % B;
+    if (j < nb) {
+      const float2* src = kspg + (s.pm[r4][j] - pt_off);
+      for (int c = tid / B; c < ncg; c += NT / B) cp_async8(&s.v[b2][j][c], src + (int64_t)c * m);
     }
     if (EXTRA) {
       if (tid < nb) {
-        if (dcf) cp_async4(&s.d[b2][tid], dcf + s.pm[r3][tid]);
+        if (dcf) cp_async4(&s.d[b2][tid], dcf + s.pm[r4][tid]);
       } else if (tid >= B && tid - B < nb) {
-        if (temporal) cp_async8(&s.t[b2][tid - B], temporal + s.pm[r3][tid - B]);
+        if (temporal) cp_async8(&s.t[b2][tid - B], temporal + s.pm[r4][tid - B]);
       }
     }
   };
-  // unit (entry j, dimension i): the K candidate taps' weights; x as a
-  // tile-aligned vector, y and z as tile-aligned vectors and as windows
+  // Candidate taps of dimension i for coordinate u: first tap lo, its cell
+  // st relative to the tile origin (wrapped), and whether the K-th candidate
+  // carries weight.
+  auto taps_of = [&](float u, int i, int& lo, int& st) {
+    const int n = sel3(gp->nos, i), size = sel3(f.size, i);
+    lo = (int)ceilf(__fsub_rn(u, sel3(kb.radius, i)));
+    st = wrap_once(lo, n) - sel3(f.org, i);
+    if (st >= size) st -= n;  // footprint wraps into this tile from the end
+  };
+  // unit (entry j, dimension i): the KW window weights, the window start, the
+  // dense flag and (x) the mask of planes with weight
   auto weights = [&](int bi) {
-    const int nb = batch_len(bi), b2 = bi & 1, r3 = bi % 3;
+    const int nb = batch_len(bi), b2 = bi & 1, r4 = bi & 3;
     // 3B units over NT threads; later rounds start at the other half of the
     // CTA, so the threads with a unit more are spread over the warps
     for (int rnd = 0; rnd * NT < 3 * B; ++rnd) {
@@ -165,57 +180,45 @@ k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
       if (t >= 3 * B) continue;
       const int j = t / 3, i = t - 3 * j;
       if (j >= nb) continue;
-      const float4 c4 = s.c[r3][j];
+      const float4 c4 = s.c[r4][j];
       const float u = i == 0 ? c4.x : (i == 1 ? c4.y : c4.z);
       const float r = sel3(kb.radius, i), ir = sel3(kb.inv_radius, i);
-      const int n = sel3(gp->nos, i), size = sel3(f.size, i);
-      const int lo = (int)ceilf(__fsub_rn(u, r));
-      int st = wrap_once(lo, n) - sel3(f.org, i);
-      if (st >= size) st -= n;  // footprint wraps into this tile from the end
-      float wq[K];
-      bool last = false;  // the K-th candidate tap carries weight
-#pragma unroll
-      for (int q = 0; q < K; ++q) {
-        const int cell = st + q;
-        const float adx = fabsf(__fsub_rn((float)(lo + q), u));
-        if (q == K - 1) last = adx <= r;
-        wq[q] = (cell >= 0 && cell < size && adx <= r) ? kb_tap_fast(adx, ir, kb) : 0.f;
-      }
-      float w[T];
-#pragma unroll
-      for (int c = 0; c < T; ++c) {
-        w[c] = 0.f;
-#pragma unroll
-        for (int q = 0; q < K; ++q)
-          if (st + q == c) w[c] = wq[q];
-      }
-      if (i == 0) {
-#pragma unroll
-        for (int c = 0; c < T; ++c) s.wx[b2][j][c] = w[c] * scale;
-        continue;
-      }
-      float* wt = i == 1 ? s.wyt[b2][j] : s.wzt[b2][j];
-      *reinterpret_cast<float4*>(wt) = make_float4(w[0], w[1], w[2], w[3]);
-      *reinterpret_cast<float4*>(wt + 4) = make_float4(w[4], w[5], w[6], w[7]);
-      // window of KW cells from w0; K taps inside the tile do not fit one
+      const int size = sel3(f.size, i);
+      int lo, st;
+      taps_of(u, i, lo, st);
+      const bool last = fabsf(__fsub_rn((float)(lo + K - 1), u)) <= r;
       const bool dense = last && st >= 0 && st + K <= size;
-      const int w0 = dense ? NW : min(max(st, 0), size - KW);
+      const int w0 = dense ? 0 : min(max(st, 0), size - KW);
       float ww[KW];
+      unsigned mask = 0;
 #pragma unroll
       for (int c = 0; c < KW; ++c) {
-        ww[c] = 0.f;
-#pragma unroll
-        for (int q = 0; q < K; ++q)
-          if (st + q == w0 + c) ww[c] = wq[q];
+        const int q = w0 + c - st;
+        const float adx = fabsf(__fsub_rn((float)(lo + q), u));
+        const bool on = q >= 0 && q < K && adx <= r;
+        ww[c] = on ? kb_tap_fast(adx, ir, kb) : 0.f;
+        mask |= on ? 1u << c : 0u;
       }
-      if (i == 1) {
+      unsigned char* cb = reinterpret_cast<unsigned char*>(&s.code[b2][j]);
+      cb[i] = (unsigned char)(w0 | (dense ? 8 : 0));
+      if (i == 0) {
+        if (dense) {  // all K candidates inside the tile
+          mask = 0;
+#pragma unroll
+          for (int q = 0; q < K; ++q)
+            if (fabsf(__fsub_rn((float)(lo + q), u)) <= r) mask |= 1u << q;
+          cb[3] = (unsigned char)(mask << st);
+        } else {
+          cb[3] = (unsigned char)(mask << w0);
+        }
+#pragma unroll
+        for (int c = 0; c < KW; ++c) s.wxw[b2][j][c] = ww[c] * scale;
+      } else if (i == 1) {
 #pragma unroll
         for (int c = 0; c < KW; ++c) s.wyw[b2][j][c] = ww[c];
-        s.code[b2][j].x = w0;
       } else {
 #pragma unroll
         for (int c = 0; c < KW; ++c) s.wzw[b2][j][c] = make_float2(ww[c], ww[c]);
-        s.code[b2][j].y = w0;
       }
     }
   };
@@ -247,16 +250,12 @@ k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
     const int b2 = bi & 1, nb = batch_len(bi);
 #pragma unroll 1
     for (int h32 = 0; h32 < B; h32 += 32) {
-      bool meet = false;
-      if (h32 + lane < nb) {
-        const float2 xw = *reinterpret_cast<const float2*>(&s.wx[b2][h32 + lane][2 * warp]);
-        meet = xw.x != 0.f || xw.y != 0.f;
-      }
+      const bool meet = h32 + lane < nb && ((s.code[b2][h32 + lane] >> (24 + 2 * warp)) & 3u) != 0u;
       unsigned act = __ballot_sync(0xffffffffu, meet);
       while (act) {
         const int j = h32 + __ffs(act) - 1;
         act &= act - 1u;
-        const float wx = s.wx[b2][j][plane];
+        const unsigned cd = s.code[b2][j];
         float2 val = has_coil ? s.v[b2][j][coil] : make_float2(0.f, 0.f);
         if (EXTRA) {
           if (dcf) {
@@ -268,9 +267,10 @@ k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
             val = make_float2(val.x * tt.x + val.y * tt.y, val.y * tt.x - val.x * tt.y);
           }
         }
-        const float2 v = __fmul2_rn(make_float2(wx, wx), val);
-        const int2 code = s.code[b2][j];
-        if (code.x < NW && code.y < NW) {  // uniform: the whole CTA shares the entry
+        if ((cd & kG3Dense) == 0u) {  // uniform: the whole CTA shares the entry
+          const int xi = plane - (int)(cd & 7u);
+          const float wx = (unsigned)xi < (unsigned)KW ? s.wxw[b2][j][xi] : 0.f;
+          const float2 v = __fmul2_rn(make_float2(wx, wx), val);
           float wy[KW];
           float2 wz[KW];
 #pragma unroll
@@ -278,22 +278,36 @@ k_grid_reg3(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KB
             wy[c] = s.wyw[b2][j][c];
             wz[c] = s.wzw[b2][j][c];
           }
-          WinDispatch<KW, NW, 0, NW * NW>::run(code.x * NW + code.y, acc, wy, wz, v);
+          WinDispatch<KW, NW, 0, NW * NW>::run((int)((cd >> 8) & 7u) * NW + (int)((cd >> 16) & 7u), acc, wy, wz, v);
         } else {
-          float wy[T];
-          float2 wz[T];
-#pragma unroll
-          for (int c = 0; c < T; ++c) {
-            wy[c] = s.wyt[b2][j][c];
-            const float z = s.wzt[b2][j][c];
-            wz[c] = make_float2(z, z);
+          // dense block: lane (dimension lane / 8, cell lane % 8) evaluates one
+          // tile-aligned weight; shuffles hand each thread its plane's x weight
+          // and every thread the y and z vectors
+          const float4 c4 = s.c[bi & 3][j];
+          float w = 0.f;
+          {
+            const int i = min(lane >> 3, 2), cell = lane & 7;
+            const float u = i == 0 ? c4.x : (i == 1 ? c4.y : c4.z);
+            int lo, st;
+            taps_of(u, i, lo, st);
+            const int q = cell - st;
+            if (cell < sel3(f.size, i) && q >= 0 && q < K) {
+              const float adx = fabsf(__fsub_rn((float)(lo + q), u));
+              if (adx <= sel3(kb.radius, i)) w = kb_tap_fast(adx, sel3(kb.inv_radius, i), kb);
+            }
           }
+          const float wx = __shfl_sync(0xffffffffu, w, plane) * scale;
+          const float2 v = __fmul2_rn(make_float2(wx, wx), val);
+          float wz[T];
+#pragma unroll
+          for (int z = 0; z < T; ++z) wz[z] = __shfl_sync(0xffffffffu, w, 16 + z);
 #pragma unroll
           for (int y = 0; y < T; ++y) {
-            if (wy[y] == 0.f) continue;  // uniform
-            const float2 v2 = __fmul2_rn(make_float2(wy[y], wy[y]), v);
+            const float wy = __shfl_sync(0xffffffffu, w, 8 + y);
+            if (wy == 0.f) continue;  // uniform
+            const float2 v2 = __fmul2_rn(make_float2(wy, wy), v);
 #pragma unroll
-            for (int z = 0; z < T; ++z) acc[y][z] = __ffma2_rn(wz[z], v2, acc[y][z]);
+            for (int z = 0; z < T; ++z) acc[y][z] = __ffma2_rn(make_float2(wz[z], wz[z]), v2, acc[y][z]);
           }
         }
       }

@@ -940,7 +940,7 @@ union G2Smem {
     int pm[3][kRegBatch];        // sample index ring
     float4 wr[2][kRegBatch][2];  // per entry: row weights x scale (cells 0-7)
     float4 wc[2][kRegBatch][4];  // per entry: column weights, each twice (cells 0-7)
-    float2 v[2][kRegBatch][CW];  // per entry and coil: sample value
+    float2 v[2][kRegBatch][CW + 1];  // per entry and coil: sample value (row padded: conflict-free copies)
     float d[2][kRegBatch];       // per entry: density weight
     float2 t[2][kRegBatch];      // per entry: temporal weight
   } b;
@@ -978,7 +978,6 @@ k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBP
   const int nos0 = gp->nos[0], nos1 = gp->nos[1];
   const Frame f = frame_of(*gp, it.tile, 2, true);
   const int64_t m = gp->m, pt_off = gp->pt_off;
-  const float2* kspc = ksp + gp->ksp_off + (int64_t)(c0 + (has_coil ? coil : 0)) * m;
   const int nbatch = (it.count + B - 1) / B;
   auto batch_len = [&](int bi) { return bi < nbatch ? min(B, it.count - bi * B) : 0; };
 
@@ -991,12 +990,19 @@ k_grid_reg(const Item* __restrict__ items, const SliceGeom* __restrict__ sl, KBP
   // values (per entry and coil), densities and temporal weights of batch bi
   auto copy_values = [&](int bi) {
     const int nb = batch_len(bi), b2 = bi & 1, r3 = bi % 3;
-    if (has_coil) {
-      if (ent_stride > 0) {  // entry-major samples: the batch's rows are contiguous
+    if (ent_stride > 0) {  // entry-major samples: the batch's rows are contiguous
+      if (has_coil) {
         const float2* eb = ksp + (int64_t)(it.start + bi * B) * ent_stride + c0 + coil;
         for (int j = sid; j < nb; j += 2 * SUB) cp_async8(&s_v[b2][j][coil], eb + (int64_t)j * ent_stride);
-      } else {
-        for (int j = sid; j < nb; j += 2 * SUB) cp_async8(&s_v[b2][j][coil], kspc + (s_pm[r3][j] - pt_off));
+      }
+    } else {
+      // thread = (entry tid % B, coil phase tid / B): one warp copy reads 16
+      // entries of each of two coil rows, i.e. consecutive samples of a row
+      // (one or two 128-byte lines) rather than 32 coil rows
+      const int j = tid % B;
+      if (j < nb) {
+        const float2* src = ksp + gp->ksp_off + (int64_t)c0 * m + (s_pm[r3][j] - pt_off);
+        for (int c = tid / B; c < ncg; c += 64 / B) cp_async8(&s_v[b2][j][c], src + (int64_t)c * m);
       }
     }
     if (tid < nb) {
