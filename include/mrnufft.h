@@ -133,6 +133,14 @@ int mrn_plan_stats(mrn_plan* plan, int64_t* out4);
  * interpolation and the gridding (contiguous rows instead of per-coil
  * gathers; the same bits). 0 skips both; set before mrn_plan_set_traj. */
 #define MRN_OPT_ENTRY_MAJOR 11
+/* MRN_OPT_NATIVE_FFT (default 1): the FFT stage as the library's own passes
+ * (one per axis, Stockham in shared memory, radices 2-5) with the apodize /
+ * zero-pad folded into the first forward pass and the crop / deapodize into
+ * the last adjoint pass, the zero-padded lines skipped; used when every slice
+ * has the same image and grid size and every grid size is a product of 2, 3
+ * and 5 of at most 1024. 0 (or any other plan) uses cuFFT between separate
+ * pad and crop kernels. The two agree to float32 rounding, not bitwise. */
+#define MRN_OPT_NATIVE_FFT 12
 int mrn_plan_set_option(mrn_plan* plan, int option, int value);
 
 /* Kaiser-Bessel beta per dimension for a raw (MRN_PLAN_RAW) plan, beta[0..ndim),

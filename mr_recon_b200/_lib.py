@@ -38,6 +38,7 @@ MRN_OPT_REG_GRIDDING = 8
 MRN_OPT_REG_INTERP = 9
 MRN_OPT_GRID_LANES = 10
 MRN_OPT_ENTRY_MAJOR = 11
+MRN_OPT_NATIVE_FFT = 12
 
 _vp = C.c_void_p
 _i = C.c_int

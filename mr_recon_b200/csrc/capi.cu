@@ -41,8 +41,7 @@ extern "C" {
 int mrn_forward(mrn_plan* P, const void* img, void* ksp, void* s) {
   RK(check_ready(P, true));
   if (!img || !ksp) return MRN_ERR_ARG;
-  { StageTimer t(P, kStagePre, ST(s)); RK(launch_pre(P, kPrePlain, (const float2*)img, nullptr, 1.0f, ST(s))); }
-  { StageTimer t(P, kStageFft, ST(s)); RK(run_fft(P, CUFFT_FORWARD, ST(s))); }
+  RK(fwd_transform(P, kPrePlain, (const float2*)img, nullptr, 1.0f, ST(s)));
   StageTimer t(P, kStageInterp, ST(s));
   return launch_interp(P, P->d_grid, kInternal, (float2*)ksp, inv_wd(P), nullptr, ST(s));
 }
@@ -51,16 +50,13 @@ int mrn_adjoint(mrn_plan* P, const void* ksp, void* img, void* s) {
   RK(check_ready(P, true));
   if (!img || !ksp) return MRN_ERR_ARG;
   { StageTimer t(P, kStageGrid, ST(s)); RK(launch_grid(P, (const float2*)ksp, nullptr, kInternal, P->d_grid, inv_wd(P), ST(s))); }
-  { StageTimer t(P, kStageFft, ST(s)); RK(run_fft(P, CUFFT_INVERSE, ST(s))); }
-  StageTimer t(P, kStagePost, ST(s));
-  return launch_post(P, kPostPlain, nullptr, (float2*)img, 1.0f, nullptr, 0.f, nullptr, 0, ST(s));
+  return inv_transform(P, (float2*)img, ST(s));
 }
 
 int mrn_forward_ft(mrn_plan* P, const void* img, void* grid, void* s) {
   if (!P || !img || !grid) return MRN_ERR_ARG;
   if (P->flags & MRN_PLAN_RAW) return MRN_ERR_UNSUPPORTED;
-  { StageTimer t(P, kStagePre, ST(s)); RK(launch_pre(P, kPrePlain, (const float2*)img, nullptr, 1.0f, ST(s))); }
-  { StageTimer t(P, kStageFft, ST(s)); RK(run_fft(P, CUFFT_FORWARD, ST(s))); }
+  RK(fwd_transform(P, kPrePlain, (const float2*)img, nullptr, 1.0f, ST(s)));
   StageTimer t(P, kStageShift, ST(s));
   return launch_shift_copy(P, P->d_grid, (float2*)grid, 1, ST(s));
 }
@@ -83,9 +79,7 @@ int mrn_adjoint_ift(mrn_plan* P, const void* grid, void* img, void* s) {
   if (!P || !img || !grid) return MRN_ERR_ARG;
   if (P->flags & MRN_PLAN_RAW) return MRN_ERR_UNSUPPORTED;
   { StageTimer t(P, kStageShift, ST(s)); RK(launch_shift_copy(P, (const float2*)grid, P->d_grid, 0, ST(s))); }
-  { StageTimer t(P, kStageFft, ST(s)); RK(run_fft(P, CUFFT_INVERSE, ST(s))); }
-  StageTimer t(P, kStagePost, ST(s));
-  return launch_post(P, kPostPlain, nullptr, (float2*)img, 1.0f, nullptr, 0.f, nullptr, 0, ST(s));
+  return inv_transform(P, (float2*)img, ST(s));
 }
 
 int mrn_traj_grad(mrn_plan* P, const void* grid, const void* samples, float* grad, float scale,
@@ -99,8 +93,7 @@ int mrn_traj_grad(mrn_plan* P, const void* grid, const void* samples, float* gra
 int mrn_sense_forward(mrn_plan* P, const void* x, const void* mps, void* ksp, void* s) {
   RK(check_ready(P, true));
   if (!x || !mps || !ksp) return MRN_ERR_ARG;
-  { StageTimer t(P, kStagePre, ST(s)); RK(launch_pre(P, kPreSense, (const float2*)x, (const float2*)mps, 1.0f, ST(s))); }
-  { StageTimer t(P, kStageFft, ST(s)); RK(run_fft(P, CUFFT_FORWARD, ST(s))); }
+  RK(fwd_transform(P, kPreSense, (const float2*)x, (const float2*)mps, 1.0f, ST(s)));
   StageTimer t(P, kStageInterp, ST(s));
   return launch_interp(P, P->d_grid, kInternal, (float2*)ksp, inv_wd(P), nullptr, ST(s));
 }
@@ -110,7 +103,7 @@ int mrn_sense_adjoint(mrn_plan* P, const void* ksp, const float* dcf, const void
   RK(check_ready(P, true));
   if (!x || !mps || !ksp) return MRN_ERR_ARG;
   { StageTimer t(P, kStageGrid, ST(s)); RK(launch_grid(P, (const float2*)ksp, dcf, kInternal, P->d_grid, inv_wd(P), ST(s))); }
-  { StageTimer t(P, kStageFft, ST(s)); RK(run_fft(P, CUFFT_INVERSE, ST(s))); }
+  RK(inv_transform(P, nullptr, ST(s)));
   StageTimer t(P, kStagePost, ST(s));
   return launch_post(P, kPostSense, (const float2*)mps, (float2*)x, out_scale, nullptr, 0.f, nullptr,
                      0, ST(s));
@@ -120,8 +113,7 @@ int mrn_sense_normal(mrn_plan* P, const void* x, const void* mps, const float* d
                      float out_scale, float lam, double* pap, int pap_stride, void* s) {
   RK(check_ready(P, true));
   if (!x || !mps || !out) return MRN_ERR_ARG;
-  { StageTimer t(P, kStagePre, ST(s)); RK(launch_pre(P, kPreSense, (const float2*)x, (const float2*)mps, 1.0f, ST(s))); }
-  { StageTimer t(P, kStageFft, ST(s)); RK(run_fft(P, CUFFT_FORWARD, ST(s))); }
+  RK(fwd_transform(P, kPreSense, (const float2*)x, (const float2*)mps, 1.0f, ST(s)));
   if (ent_path_ok(P)) {
     // 2D: the samples between the two stages in gridding-entry order, with the
     // density weight applied by the interpolation (the same products, so the
@@ -139,7 +131,7 @@ int mrn_sense_normal(mrn_plan* P, const void* x, const void* mps, const float* d
     { StageTimer t(P, kStageInterp, ST(s)); RK(launch_interp(P, P->d_grid, kInternal, P->d_ksp_tmp, inv_wd(P), nullptr, ST(s))); }
     { StageTimer t(P, kStageGrid, ST(s)); RK(launch_grid(P, P->d_ksp_tmp, dcf, kInternal, P->d_grid, inv_wd(P), ST(s))); }
   }
-  { StageTimer t(P, kStageFft, ST(s)); RK(run_fft(P, CUFFT_INVERSE, ST(s))); }
+  RK(inv_transform(P, nullptr, ST(s)));
   StageTimer t(P, kStagePost, ST(s));
   return launch_post(P, kPostSense, (const float2*)mps, (float2*)out, out_scale, (const float2*)x,
                      lam, pap, pap_stride, ST(s));

@@ -43,6 +43,8 @@ struct SliceGeom {
   int64_t irow_off;      // first image row (all coils) of the slice
   int64_t xrow_off;      // first image row of the one-image-per-slice layout
   float inv_sqrt_n;      // 1 / sqrt(prod(n)) (fourier.py:462, 522)
+  int native_fft;        // the slice's FFT group runs the native passes (ffx.cu),
+                         // which pad and crop it themselves
 };
 
 // Work item: one tile (or a chunk of a heavy tile) of one slice. Item lists
@@ -86,6 +88,20 @@ struct EntIO {
 };
 
 constexpr int kKBTerms = 32;  // terms of the I0 power series kept in KBParams
+
+// One axis of the native FFT (ffx.cu): length n = radix[0] * ... *
+// radix[ns - 1], each radix 2, 3, 4 or 5; stage s reads its twiddles
+// exp(-2 pi i t j / (L R)), j < L = radix[0] * ... * radix[s - 1], 1 <= t < R,
+// at tw + tw_off[s] + j (R - 1) + t - 1 of the axis' table (n - 1 entries).
+constexpr int kFfxMaxStages = 12;
+constexpr int kFfxMaxN = 1024;
+struct FfxAxis {
+  int n;
+  int ns;
+  int radix[kFfxMaxStages];
+  int tw_off[kFfxMaxStages];
+  int tw_base;  // first entry of this axis in the plan's twiddle table
+};
 
 struct KBParams {
   float radius[kMaxDim];  // W_i / 2
@@ -288,6 +304,18 @@ __host__ __device__ __forceinline__ int tile_of(int s, int nos, int nt) {
   return (int)((((int64_t)s + 1) * nt - 1) / nos);
 }
 
+// Slice of a global row index: which 0 = grid rows (prow_off), 1 = image
+// rows (irow_off), 2 = one-image-per-slice rows (xrow_off).
+__device__ __forceinline__ int slice_by_row(const SliceGeom* sl, int ns, int64_t row, int which) {
+  int lo = 0, hi = ns - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    const int64_t o = which == 0 ? sl[mid].prow_off : (which == 1 ? sl[mid].irow_off : sl[mid].xrow_off);
+    if (o <= row) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
 }  // namespace mrn
 
 // Host-side plan object (defined in plan.cu).
@@ -401,6 +429,26 @@ struct mrn_plan {
     cufftHandle handle;
   };
   std::vector<FftGroup> fft;
+  // Native FFT (ffx.cu), per FFT group: used for a group whose slices have
+  // the same image size and whose grid axes factor into radices 2-5 with at
+  // most kFfxMaxN points; other groups keep cuFFT. MRN_OPT_NATIVE_FFT
+  // selects it (default) or cuFFT for every group.
+  struct FfxGroup {
+    bool native;      // the group's axes and slices qualify
+    mrn::FfxAxis ax[mrn::kMaxDim];
+    int first_slice;  // geometry (image and grid size) shared by the group's slices
+    int nsl;          // slices in the group
+    int sl_off;       // their ids at d_ffx_sl + sl_off, in grid order
+    int row_off;      // first grid row of each at d_ffx_row + row_off (nsl + 1 entries)
+    int64_t nrows;    // grid rows (coils x all axes but the last) of the group
+  };
+  bool ffx_ok = false;   // some group is native
+  bool ffx_all = false;  // every group is native
+  bool use_ffx = true;
+  std::vector<FfxGroup> ffx;
+  float2* d_ffx_tw = nullptr;   // twiddle tables of every group's axes, back to back
+  int* d_ffx_sl = nullptr;
+  int64_t* d_ffx_row = nullptr;
 
   // Optional stage timing (mrn_plan_enable_timing): CUDA event pairs recorded
   // on the launching stream around each stage, summed by mrn_plan_timing.

@@ -18,16 +18,6 @@
 
 namespace mrn {
 
-__device__ __forceinline__ int slice_by_row(const SliceGeom* sl, int ns, int64_t row, int which) {
-  int lo = 0, hi = ns - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    const int64_t o = which == 0 ? sl[mid].prow_off : (which == 1 ? sl[mid].irow_off : sl[mid].xrow_off);
-    if (o <= row) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
-
 // One warp per grid row (all dims but the last) of one coil of one slice.
 template <int D>
 __global__ void __launch_bounds__(256)
@@ -39,6 +29,7 @@ k_pre(const SliceGeom* __restrict__ sl, int ns, const float* __restrict__ apod,
   if (row >= nrows) return;
   const int s = slice_by_row(sl, ns, row, 0);
   const SliceGeom& g = sl[s];
+  if (g.native_fft) return;  // padded by the native forward pass
   const int64_t r = row - g.prow_off;
   const int64_t outer = g.gos / g.nos[D - 1];
   const int c = (int)(r / outer);
@@ -137,6 +128,7 @@ __device__ __forceinline__ void post_row(const SliceGeom* __restrict__ sl, int n
                                          double* __restrict__ rowpart, int64_t row, int lane) {
   const int s = slice_by_row(sl, ns, row, mode == kPostSense ? 2 : 1);
   const SliceGeom& g = sl[s];
+  if (mode == kPostPlain && g.native_fft) return;  // cropped by the native inverse pass
   const int64_t r = row - (mode == kPostSense ? g.xrow_off : g.irow_off);
   const int64_t outer = g.nimg / g.n[D - 1];
   const int c_plain = mode == kPostSense ? 0 : (int)(r / outer);
@@ -377,8 +369,49 @@ int launch_shift_copy(mrn_plan* P, const float2* src, float2* dst, int to_user, 
   return e == cudaSuccess ? MRN_OK : cuda_fail(e);
 }
 
-int run_fft(mrn_plan* P, int direction, cudaStream_t st) {
-  for (auto& fg : P->fft) {
+int fwd_transform(mrn_plan* P, PreMode mode, const float2* src, const float2* mps, float scale,
+                  cudaStream_t st) {
+  if (ffx_active(P)) {
+    StageTimer t(P, kStageFft, st);
+    if (!P->ffx_all) {  // groups left to cuFFT: pad them (k_pre skips native slices) and transform
+      int rc = launch_pre(P, mode, src, mps, scale, st);
+      if (rc == MRN_OK) rc = run_fft(P, CUFFT_FORWARD, st, true);
+      if (rc != MRN_OK) return rc;
+    }
+    return ffx_forward(P, mode, src, mps, scale, st);
+  }
+  {
+    StageTimer t(P, kStagePre, st);
+    const int rc = launch_pre(P, mode, src, mps, scale, st);
+    if (rc != MRN_OK) return rc;
+  }
+  StageTimer t(P, kStageFft, st);
+  return run_fft(P, CUFFT_FORWARD, st);
+}
+
+int inv_transform(mrn_plan* P, float2* out, cudaStream_t st) {
+  if (ffx_active(P)) {
+    StageTimer t(P, kStageFft, st);
+    int rc = ffx_inverse(P, out, 1.0f, st);
+    if (rc != MRN_OK || P->ffx_all) return rc;
+    rc = run_fft(P, CUFFT_INVERSE, st, true);  // k_post then skips native slices
+    if (rc != MRN_OK || !out) return rc;
+    return launch_post(P, kPostPlain, nullptr, out, 1.0f, nullptr, 0.f, nullptr, 0, st);
+  }
+  {
+    StageTimer t(P, kStageFft, st);
+    const int rc = run_fft(P, CUFFT_INVERSE, st);
+    if (rc != MRN_OK) return rc;
+  }
+  if (!out) return MRN_OK;
+  StageTimer t(P, kStagePost, st);
+  return launch_post(P, kPostPlain, nullptr, out, 1.0f, nullptr, 0.f, nullptr, 0, st);
+}
+
+int run_fft(mrn_plan* P, int direction, cudaStream_t st, bool skip_native) {
+  for (size_t q = 0; q < P->fft.size(); ++q) {
+    auto& fg = P->fft[q];
+    if (skip_native && q < P->ffx.size() && P->ffx[q].native) continue;
     if (cufftSetStream(fg.handle, st) != CUFFT_SUCCESS) return MRN_ERR_CUFFT;
     cufftComplex* p = reinterpret_cast<cufftComplex*>(P->d_grid + fg.grid_off);
     if (cufftExecC2C(fg.handle, p, p, direction) != CUFFT_SUCCESS) return MRN_ERR_CUFFT;

@@ -1,0 +1,603 @@
+// Native FFT stage of the NUFFT: the d-dimensional C2C transform of the
+// plan's oversampled grid as one pass per axis, with the NUFFT's zero padding
+// and cropping folded into the passes.
+//
+// Reference: fourier.py (:470-560) apodizes and pads the image into the
+// oversampled grid (centred pad + ifftshift), calls torch.fft.fftn, and on
+// the adjoint calls ifftn and crops (norm=None: unnormalised transforms; the
+// 1/sqrt(prod N) and the apodization are applied in the first forward / last
+// adjoint pass with the same float products as k_pre / k_post).
+//
+// Passes. Forward: the last axis first, one warp per grid line, fused with the
+// apodize / pad: a line whose outer storage indices fall in the zero padding
+// is all zero and is neither computed nor stored. Then every other axis from
+// the last-but-one to the first, a CTA per block of W adjacent columns: rows
+// of the axis inside its zero padding read as zero, and the planes whose
+// (untransformed) earlier-axis index lies in the padding are skipped.
+// Adjoint: the first axis first (every row read, only the rows that survive
+// the crop stored), the middle axis on the surviving planes likewise, and
+// the last axis as a warp per surviving line fused with the crop /
+// deapodize, or stored back in place for the SENSE coil combination, which
+// reads only surviving lines.
+//
+// Each line is a Stockham autosort FFT in shared memory: stage s with radix R
+// and L = the product of the earlier radices maps butterfly b = k L + j
+// (j < L) to out[k R L + u L + j] = sum_t x[b + t n / R] w^(t j)
+// e^(-+2 pi i t u / R), w = e^(-+2 pi i / (L R)) (radices 4, 5, 3, 2); the
+// twiddles come from a table computed on the host in double precision. The
+// result is in natural order after the last stage, with no bit reversal.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "internal.cuh"
+#include "tile_util.cuh"
+
+namespace mrn {
+
+namespace {
+
+constexpr float kSin3 = 0.866025403784438647f;   // sin(2 pi / 3)
+constexpr float kCos51 = 0.309016994374947424f;  // cos(2 pi / 5)
+constexpr float kCos52 = -0.809016994374947424f; // cos(4 pi / 5)
+constexpr float kSin51 = 0.951056516295153572f;  // sin(2 pi / 5)
+constexpr float kSin52 = 0.587785252292473129f;  // sin(4 pi / 5)
+constexpr int kFfxThreads = 256;
+constexpr int kFfxCols = 8;  // adjacent columns per CTA in the strided passes
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
+// a w (forward) or a conj(w) (inverse)
+template <bool INV>
+__device__ __forceinline__ float2 ctw(float2 a, float2 w) {
+  return INV ? make_float2(a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y)
+             : make_float2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);
+}
+
+// c (-i a) (forward) or c (+i a) (inverse)
+template <bool INV>
+__device__ __forceinline__ float2 rot(float2 a, float c) {
+  return INV ? make_float2(-c * a.y, c * a.x) : make_float2(c * a.y, -c * a.x);
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void dft(float2 (&x)[R]) {
+  if constexpr (R == 2) {
+    const float2 a = x[0];
+    x[0] = cadd(a, x[1]);
+    x[1] = csub(a, x[1]);
+  } else if constexpr (R == 3) {
+    const float2 s = cadd(x[1], x[2]);
+    const float2 m = make_float2(x[0].x - 0.5f * s.x, x[0].y - 0.5f * s.y);
+    const float2 d = rot<INV>(csub(x[1], x[2]), kSin3);
+    x[0] = cadd(x[0], s);
+    x[1] = cadd(m, d);
+    x[2] = csub(m, d);
+  } else if constexpr (R == 4) {
+    const float2 a0 = cadd(x[0], x[2]), a1 = csub(x[0], x[2]);
+    const float2 a2 = cadd(x[1], x[3]), a3 = rot<INV>(csub(x[1], x[3]), 1.0f);
+    x[0] = cadd(a0, a2);
+    x[2] = csub(a0, a2);
+    x[1] = cadd(a1, a3);
+    x[3] = csub(a1, a3);
+  } else {  // R == 5
+    const float2 a1 = cadd(x[1], x[4]), b1 = csub(x[1], x[4]);
+    const float2 a2 = cadd(x[2], x[3]), b2 = csub(x[2], x[3]);
+    const float2 r1 = make_float2(x[0].x + kCos51 * a1.x + kCos52 * a2.x, x[0].y + kCos51 * a1.y + kCos52 * a2.y);
+    const float2 r2 = make_float2(x[0].x + kCos52 * a1.x + kCos51 * a2.x, x[0].y + kCos52 * a1.y + kCos51 * a2.y);
+    const float2 p1 = rot<INV>(make_float2(kSin51 * b1.x + kSin52 * b2.x, kSin51 * b1.y + kSin52 * b2.y), 1.0f);
+    const float2 p2 = rot<INV>(make_float2(kSin52 * b1.x - kSin51 * b2.x, kSin52 * b1.y - kSin51 * b2.y), 1.0f);
+    x[0] = cadd(x[0], cadd(a1, a2));
+    x[1] = cadd(r1, p1);
+    x[4] = csub(r1, p1);
+    x[2] = cadd(r2, p2);
+    x[3] = csub(r2, p2);
+  }
+}
+
+// Butterfly bi of a stage (radix R, L, n / R = nr) over elements es apart.
+template <int R, bool INV>
+__device__ __forceinline__ void bfly(const float2* __restrict__ a, float2* __restrict__ b, int L, int nr,
+                                     const float2* __restrict__ tw, int bi, int es) {
+  const int k = bi / L, j = bi - k * L;
+  float2 x[R];
+#pragma unroll
+  for (int t = 0; t < R; ++t) x[t] = a[(bi + t * nr) * es];
+  if (j > 0) {
+#pragma unroll
+    for (int t = 1; t < R; ++t) x[t] = ctw<INV>(x[t], tw[j * (R - 1) + t - 1]);
+  }
+  dft<R, INV>(x);
+  const int ob = k * R * L + j;
+#pragma unroll
+  for (int u = 0; u < R; ++u) b[(ob + u * L) * es] = x[u];
+}
+
+template <bool INV>
+__device__ __forceinline__ void bfly_any(int R, const float2* a, float2* b, int L, int nr, const float2* tw,
+                                         int bi, int es) {
+  switch (R) {
+    case 4: bfly<4, INV>(a, b, L, nr, tw, bi, es); break;
+    case 5: bfly<5, INV>(a, b, L, nr, tw, bi, es); break;
+    case 3: bfly<3, INV>(a, b, L, nr, tw, bi, es); break;
+    default: bfly<2, INV>(a, b, L, nr, tw, bi, es); break;
+  }
+}
+
+// Axis plan in shared memory (kernel parameters indexed at run time would go
+// through local memory).
+struct FfxShared {
+  int radix[kFfxMaxStages];
+  int tw_off[kFfxMaxStages];
+};
+
+__device__ __forceinline__ void stage_axis(FfxShared& sa, float2* tw, const FfxAxis& ax,
+                                           const float2* __restrict__ twg) {
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < kFfxMaxStages; ++i) {
+      sa.radix[i] = ax.radix[i];
+      sa.tw_off[i] = ax.tw_off[i];
+    }
+  }
+  for (int i = threadIdx.x; i < ax.n - 1; i += blockDim.x) tw[i] = twg[ax.tw_base + i];
+}
+
+// One line of n points by one warp: a holds the input, b is scratch; returns
+// the buffer that holds the transform.
+template <bool INV>
+__device__ __forceinline__ float2* line_fft(float2* a, float2* b, int n, int ns, const FfxShared& sa,
+                                            const float2* tw, int lane) {
+  int L = 1;
+  for (int s = 0; s < ns; ++s) {
+    const int R = sa.radix[s], nr = n / R;
+    const float2* t = tw + sa.tw_off[s];
+    for (int bi = lane; bi < nr; bi += 32) bfly_any<INV>(R, a, b, L, nr, t, bi, 1);
+    __syncwarp();
+    float2* tmp = a;
+    a = b;
+    b = tmp;
+    L *= R;
+  }
+  return a;
+}
+
+// Slice k of the group holding group row `row` (grow: first row of each of
+// the gns slices, then the total).
+__device__ __forceinline__ void row_slice(const int64_t* __restrict__ grow, int gns, int64_t row, int& k) {
+  int lo = 0, hi = gns - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (grow[mid] <= row) lo = mid; else hi = mid - 1;
+  }
+  k = lo;
+}
+
+// index i of an axis of n image points in nos grid points survives the crop
+// (is not zero padding): the image index (i + n / 2) mod nos is below n
+__device__ __forceinline__ bool kept(int i, int n, int nos) {
+  int q = i + n / 2;
+  if (q >= nos) q -= nos;
+  return q < n;
+}
+
+// Forward pass over the last axis fused with the apodize / pad (k_pre's
+// products): one warp per grid row (slice, coil, outer storage index).
+template <int D, bool SENSE>
+__global__ void __launch_bounds__(kFfxThreads)
+k_ffx_rows_fwd(const SliceGeom* __restrict__ sl, const int* __restrict__ gsl, const int64_t* __restrict__ grow,
+               int gns, const float* __restrict__ apod, const float2* __restrict__ src,
+               const float2* __restrict__ mps, float scale, float2* __restrict__ grid, int64_t nrows, FfxAxis ax,
+               const float2* __restrict__ twg) {
+  extern __shared__ float2 fsm[];
+  __shared__ FfxShared sa;
+  const int n = ax.n, nw = blockDim.x >> 5;
+  float2* tw = fsm;
+  stage_axis(sa, tw, ax, twg);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t row = (int64_t)blockIdx.x * nw + warp;
+  if (row >= nrows) return;
+  int k = 0;
+  row_slice(grow, gns, row, k);
+  const SliceGeom& g = sl[gsl[k]];
+  const int64_t r = row - grow[k];
+  const int64_t outer = g.gos / n;
+  const int c = (int)(r / outer);
+  int64_t o = r - (int64_t)c * outer;
+  const int64_t lrow = o;
+  float aout = scale * g.inv_sqrt_n;
+  int st[kMaxDim] = {0, 0, 0};
+  for (int i = D - 2; i >= 0; --i) {
+    st[i] = (int)(o % g.nos[i]);
+    o /= g.nos[i];
+  }
+  int64_t qlin = 0;
+  for (int i = 0; i < D - 1; ++i) {
+    int q = st[i] + g.n[i] / 2;
+    if (q >= g.nos[i]) q -= g.nos[i];
+    if (q >= g.n[i]) return;  // zero padding: the line stays zero and is never read
+    aout *= apod[g.apod_off[i] + q];
+    qlin = qlin * g.n[i] + q;
+  }
+  const int nl = g.n[D - 1], h = nl / 2;
+  qlin *= nl;
+  const float* al = apod + g.apod_off[D - 1];
+  const float2* srow = SENSE ? src + g.x_off + qlin : src + g.img_off + (int64_t)c * g.nimg + qlin;
+  const float2* mrow = SENSE ? mps + g.img_off + (int64_t)c * g.nimg + qlin : nullptr;
+  float2* A = fsm + n + warp * 2 * n;
+  float2* B = A + n;
+#pragma unroll 4
+  for (int j = lane; j < n; j += 32) {
+    int q = j + h;
+    if (q >= n) q -= n;
+    float2 v = make_float2(0.f, 0.f);
+    if (q < nl) {
+      float2 x = __ldg(srow + q);
+      if (SENSE) {
+        const float2 m = __ldg(mrow + q);
+        x = make_float2(x.x * m.x - x.y * m.y, x.x * m.y + x.y * m.x);
+      }
+      const float a = aout * al[q];
+      v = make_float2(x.x * a, x.y * a);
+    }
+    A[j] = v;
+  }
+  __syncwarp();
+  const float2* res = line_fft<false>(A, B, n, ax.ns, sa, tw, lane);
+  float2* dst = grid + g.grid_off + (int64_t)c * g.gos + lrow * n;
+#pragma unroll 4
+  for (int j = lane; j < n; j += 32) dst[j] = res[j];
+}
+
+// Inverse pass over the last axis of the rows that survive the crop: POST
+// crops and deapodizes into the image (k_post's products), else the row is
+// stored back for the SENSE coil combination.
+template <int D, bool POST>
+__global__ void __launch_bounds__(kFfxThreads)
+k_ffx_rows_inv(const SliceGeom* __restrict__ sl, const int* __restrict__ gsl, const int64_t* __restrict__ grow,
+               int gns, const float* __restrict__ apod, float2* __restrict__ grid, float scale,
+               float2* __restrict__ out, int64_t nrows, FfxAxis ax, const float2* __restrict__ twg) {
+  extern __shared__ float2 fsm[];
+  __shared__ FfxShared sa;
+  const int n = ax.n, nw = blockDim.x >> 5;
+  float2* tw = fsm;
+  stage_axis(sa, tw, ax, twg);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t row = (int64_t)blockIdx.x * nw + warp;
+  if (row >= nrows) return;
+  int k = 0;
+  row_slice(grow, gns, row, k);
+  const SliceGeom& g = sl[gsl[k]];
+  const int64_t r = row - grow[k];
+  const int64_t outer = g.gos / n;
+  const int c = (int)(r / outer);
+  int64_t o = r - (int64_t)c * outer;
+  const int64_t lrow = o;
+  int st[kMaxDim] = {0, 0, 0};
+  for (int i = D - 2; i >= 0; --i) {
+    st[i] = (int)(o % g.nos[i]);
+    o /= g.nos[i];
+  }
+  float aout = scale * g.inv_sqrt_n;
+  int64_t qlin = 0;
+  for (int i = 0; i < D - 1; ++i) {
+    int q = st[i] + g.n[i] / 2;
+    if (q >= g.nos[i]) q -= g.nos[i];
+    if (q >= g.n[i]) return;  // cropped away
+    aout *= apod[g.apod_off[i] + q];
+    qlin = qlin * g.n[i] + q;
+  }
+  float2* gline = grid + g.grid_off + (int64_t)c * g.gos + lrow * n;
+  float2* A = fsm + n + warp * 2 * n;
+  float2* B = A + n;
+#pragma unroll 4
+  for (int j = lane; j < n; j += 32) A[j] = gline[j];
+  __syncwarp();
+  const float2* res = line_fft<true>(A, B, n, ax.ns, sa, tw, lane);
+  if (!POST) {
+#pragma unroll 4
+    for (int j = lane; j < n; j += 32) gline[j] = res[j];
+    return;
+  }
+  const int nl = g.n[D - 1], h = nl / 2;
+  const float* al = apod + g.apod_off[D - 1];
+  float2* orow = out + g.img_off + (int64_t)c * g.nimg + qlin * nl;
+#pragma unroll 4
+  for (int j = lane; j < nl; j += 32) {
+    int sj = j - h;
+    if (sj < 0) sj += n;
+    const float2 y = res[sj];
+    const float a = aout * al[j];
+    orow[j] = make_float2(y.x * a, y.y * a);
+  }
+}
+
+// One strided axis: the grid as [outer][n][stride] (stride = product of the
+// later axes' sizes), a CTA per (outer index, block of W adjacent columns).
+// Forward: rows in the axis' zero padding read as zero; inverse: only rows
+// that survive the crop are stored. skip_nos > 0: the outer index's
+// earlier-axis coordinate (outer mod skip_nos) must survive the crop (its
+// plane is zero padding in the forward direction, unused in the inverse).
+template <bool INV, int W>
+__global__ void __launch_bounds__(kFfxThreads)
+k_ffx_cols(float2* __restrict__ grid, FfxAxis ax, const float2* __restrict__ twg, int64_t stride,
+           int64_t nib, int n_img, int skip_n, int skip_nos) {
+  const int64_t blk = blockIdx.x;
+  const int64_t o = blk / nib, ib = blk - o * nib;
+  if (skip_nos > 0 && !kept((int)(o % skip_nos), skip_n, skip_nos)) return;  // whole CTA
+  extern __shared__ float2 fsm[];
+  __shared__ FfxShared sa;
+  const int n = ax.n, tid = threadIdx.x;
+  float2* tw = fsm;
+  float2* A = fsm + n;
+  float2* B = A + n * W;
+  stage_axis(sa, tw, ax, twg);
+  const int64_t w0 = ib * W;
+  const int wn = (int)min((int64_t)W, stride - w0);
+  float2* base = grid + o * n * stride + w0;
+  for (int idx = tid; idx < n * W; idx += kFfxThreads) {
+    const int rr = idx / W, w = idx - rr * W;
+    if (w < wn && (INV || kept(rr, n_img, n))) cp_async8(&A[idx], base + rr * stride + w);
+    else A[idx] = make_float2(0.f, 0.f);
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  int L = 1;
+  for (int s = 0; s < ax.ns; ++s) {
+    const int R = sa.radix[s], nr = n / R;
+    const float2* t = tw + sa.tw_off[s];
+    for (int idx = tid; idx < nr * W; idx += kFfxThreads) {
+      const int bi = idx / W, w = idx - bi * W;
+      bfly_any<INV>(R, A + w, B + w, L, nr, t, bi, W);
+    }
+    __syncthreads();
+    float2* tmp = A;
+    A = B;
+    B = tmp;
+    L *= R;
+  }
+  for (int idx = tid; idx < n * W; idx += kFfxThreads) {
+    const int rr = idx / W, w = idx - rr * W;
+    if (w < wn && (!INV || kept(rr, n_img, n))) base[rr * stride + w] = A[idx];
+  }
+}
+
+int rows_warps(int n) {
+  // twiddles + two buffers of n points per warp within 48 KB
+  const int w = (int)((48 * 1024 / sizeof(float2) - n) / (2 * n));
+  return std::max(1, std::min(8, w));
+}
+
+int launch_cols(mrn_plan* P, int q, int a, bool inv, cudaStream_t st) {
+  const int D = P->ndim;
+  const mrn_plan::FfxGroup& fg = P->ffx[q];
+  const SliceGeom& g = P->h_slices[fg.first_slice];
+  const FfxAxis& ax = fg.ax[a];
+  int64_t stride = 1, outer = P->fft[q].batch;
+  for (int i = a + 1; i < D; ++i) stride *= g.nos[i];
+  for (int i = 0; i < a; ++i) outer *= g.nos[i];
+  constexpr int W = kFfxCols;
+  const int64_t nib = (stride + W - 1) / W;
+  const int64_t nblocks = outer * nib;
+  if (nblocks <= 0) return MRN_OK;
+  if (nblocks > 0x7fffffffLL) return MRN_ERR_UNSUPPORTED;
+  const size_t smem = ((size_t)ax.n + 2 * (size_t)ax.n * W) * sizeof(float2);
+  const int skip_n = a == 1 ? g.n[0] : 0, skip_nos = a == 1 ? g.nos[0] : 0;
+  float2* grid = P->d_grid + P->fft[q].grid_off;
+  int rc;
+  if (inv) {
+    auto kern = k_ffx_cols<true, W>;
+    rc = set_dynamic_smem(kern, smem);
+    if (rc == MRN_OK)
+      kern<<<(unsigned)nblocks, kFfxThreads, smem, st>>>(grid, ax, P->d_ffx_tw, stride, nib, g.n[a], skip_n, skip_nos);
+  } else {
+    auto kern = k_ffx_cols<false, W>;
+    rc = set_dynamic_smem(kern, smem);
+    if (rc == MRN_OK)
+      kern<<<(unsigned)nblocks, kFfxThreads, smem, st>>>(grid, ax, P->d_ffx_tw, stride, nib, g.n[a], skip_n, skip_nos);
+  }
+  if (rc != MRN_OK) return rc;
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? MRN_OK : cuda_fail(e);
+}
+
+// Radices for n (4 first, then 5, 3, 2); false if n has another prime factor.
+bool ffx_factor(int n, FfxAxis& ax) {
+  ax = FfxAxis{};
+  ax.n = n;
+  if (n < 2 || n > kFfxMaxN) return false;
+  int m = n, s = 0;
+  for (int r : {4, 5, 3, 2}) {
+    while (m % r == 0) {
+      if (s == kFfxMaxStages) return false;
+      ax.radix[s++] = r;
+      m /= r;
+    }
+  }
+  ax.ns = s;
+  return m == 1;
+}
+
+template <class T>
+int upload(T** dst, const std::vector<T>& v) {
+  if (*dst) cudaFree(*dst);
+  *dst = nullptr;
+  if (cudaMalloc(dst, std::max<size_t>(1, v.size()) * sizeof(T)) != cudaSuccess) return MRN_ERR_CUDA;
+  if (!v.empty() && cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+    return MRN_ERR_CUDA;
+  return MRN_OK;
+}
+
+}  // namespace
+
+bool ffx_active(const mrn_plan* P) { return P->ffx_ok && P->use_ffx; }
+
+// Per-slice flags: the slice's group runs the native passes (and k_pre /
+// k_post leave it alone).
+int ffx_refresh(mrn_plan* P) {
+  if (P->h_slices.empty() || !P->d_slices) return MRN_OK;
+  const int D = P->ndim;
+  for (auto& g : P->h_slices) {
+    g.native_fft = 0;
+    if (!P->use_ffx) continue;
+    for (const auto& fg : P->ffx) {
+      bool same = fg.native;
+      for (int i = 0; i < D && same; ++i) same = g.nos[i] == fg.ax[i].n;
+      if (same) g.native_fft = 1;
+    }
+  }
+  return upload_slices(P) == cudaSuccess ? MRN_OK : MRN_ERR_CUDA;
+}
+
+// Decide, per FFT group, whether the native FFT applies and build its axes'
+// twiddle tables and its slice / row lists (plan creation, after the FFT
+// groups exist). A group whose slices differ in image size, or with an axis
+// that has a prime factor above 5 or more than kFfxMaxN points, keeps cuFFT.
+int ffx_setup(mrn_plan* P) {
+  P->ffx_ok = P->ffx_all = false;
+  P->ffx.clear();
+  if ((P->flags & MRN_PLAN_RAW) || (P->ndim != 2 && P->ndim != 3) || P->h_slices.empty()) return MRN_OK;
+  const int D = P->ndim;
+  std::vector<float2> tab;
+  std::vector<int> sl_ids;
+  std::vector<int64_t> rows;
+  int nnative = 0;
+  for (size_t q = 0; q < P->fft.size(); ++q) {
+    mrn_plan::FfxGroup fg{};
+    fg.native = true;
+    fg.first_slice = -1;
+    fg.sl_off = (int)sl_ids.size();
+    fg.row_off = (int)rows.size();
+    int64_t r = 0;
+    for (int s = 0; s < (int)P->h_slices.size(); ++s) {
+      const SliceGeom& g = P->h_slices[s];
+      bool same = true;
+      for (int i = 0; i < D; ++i) same &= g.nos[i] == P->fft[q].nos[i];
+      if (!same) continue;
+      if (fg.first_slice < 0) fg.first_slice = s;
+      const SliceGeom& g0 = P->h_slices[fg.first_slice];
+      for (int i = 0; i < D; ++i) fg.native &= g.n[i] == g0.n[i];
+      sl_ids.push_back(s);
+      rows.push_back(r);
+      r += (int64_t)g.ncoil * (g.gos / g.nos[D - 1]);
+      ++fg.nsl;
+    }
+    rows.push_back(r);
+    fg.nrows = r;
+    for (int i = 0; i < D; ++i) {
+      FfxAxis& ax = fg.ax[i];
+      if (!ffx_factor(P->fft[q].nos[i], ax)) {
+        fg.native = false;
+        continue;
+      }
+      ax.tw_base = (int)tab.size();
+      int L = 1, off = 0;
+      for (int s = 0; s < ax.ns; ++s) {
+        const int R = ax.radix[s];
+        ax.tw_off[s] = off;
+        for (int j = 0; j < L; ++j)
+          for (int t = 1; t < R; ++t) {
+            const double ang = -2.0 * M_PI * (double)t * (double)j / (double)(L * R);
+            tab.push_back(make_float2((float)std::cos(ang), (float)std::sin(ang)));
+          }
+        off += L * (R - 1);
+        L *= R;
+      }
+    }
+    nnative += fg.native ? 1 : 0;
+    P->ffx.push_back(fg);
+  }
+  if (nnative == 0) {
+    P->ffx.clear();
+    return MRN_OK;
+  }
+  int rc = upload(&P->d_ffx_tw, tab);
+  if (rc == MRN_OK) rc = upload(&P->d_ffx_sl, sl_ids);
+  if (rc == MRN_OK) rc = upload(&P->d_ffx_row, rows);
+  if (rc != MRN_OK) return rc;
+  P->ffx_ok = true;
+  P->ffx_all = nnative == (int)P->fft.size();
+  return ffx_refresh(P);
+}
+
+// Apodize / pad (plain image or SENSE x * maps) and forward FFT of the grid.
+int ffx_forward(mrn_plan* P, PreMode mode, const float2* src, const float2* mps, float scale, cudaStream_t st) {
+  const int D = P->ndim;
+  const bool sense = mode == kPreSense;
+  for (size_t q = 0; q < P->ffx.size(); ++q) {
+    const mrn_plan::FfxGroup& fg = P->ffx[q];
+    if (!fg.native) continue;
+    const FfxAxis& ax = fg.ax[D - 1];
+    const int nw = rows_warps(ax.n);
+    const unsigned blocks = (unsigned)((fg.nrows + nw - 1) / nw);
+    const size_t smem = ((size_t)ax.n + 2 * (size_t)nw * ax.n) * sizeof(float2);
+    const int* gsl = P->d_ffx_sl + fg.sl_off;
+    const int64_t* grow = P->d_ffx_row + fg.row_off;
+    int rc = MRN_OK;
+    if (blocks > 0) {
+#define MRN_FFX_ROWS(DD, SS)                                                                       \
+  do {                                                                                             \
+    auto kern = k_ffx_rows_fwd<DD, SS>;                                                            \
+    rc = set_dynamic_smem(kern, smem);                                                             \
+    if (rc == MRN_OK)                                                                              \
+      kern<<<blocks, nw * 32, smem, st>>>(P->d_slices, gsl, grow, fg.nsl, P->d_apod, src, mps, scale, \
+                                          P->d_grid, fg.nrows, ax, P->d_ffx_tw);                   \
+  } while (0)
+      if (D == 2) { if (sense) MRN_FFX_ROWS(2, true); else MRN_FFX_ROWS(2, false); }
+      else { if (sense) MRN_FFX_ROWS(3, true); else MRN_FFX_ROWS(3, false); }
+#undef MRN_FFX_ROWS
+      if (rc != MRN_OK) return rc;
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_fail(e);
+    }
+    for (int a = D - 2; a >= 0; --a) {
+      rc = launch_cols(P, (int)q, a, false, st);
+      if (rc != MRN_OK) return rc;
+    }
+  }
+  return MRN_OK;
+}
+
+// Inverse FFT of the grid; out != nullptr: crop / deapodize into the image
+// batch (plain adjoint), else the surviving lines stay in the grid.
+int ffx_inverse(mrn_plan* P, float2* out, float scale, cudaStream_t st) {
+  const int D = P->ndim;
+  for (size_t q = 0; q < P->ffx.size(); ++q) {
+    const mrn_plan::FfxGroup& fg = P->ffx[q];
+    if (!fg.native) continue;
+    int rc = MRN_OK;
+    for (int a = 0; a <= D - 2; ++a) {
+      rc = launch_cols(P, (int)q, a, true, st);
+      if (rc != MRN_OK) return rc;
+    }
+    const FfxAxis& ax = fg.ax[D - 1];
+    const int nw = rows_warps(ax.n);
+    const unsigned blocks = (unsigned)((fg.nrows + nw - 1) / nw);
+    if (blocks == 0) continue;
+    const size_t smem = ((size_t)ax.n + 2 * (size_t)nw * ax.n) * sizeof(float2);
+    const int* gsl = P->d_ffx_sl + fg.sl_off;
+    const int64_t* grow = P->d_ffx_row + fg.row_off;
+#define MRN_FFX_IROWS(DD, PP)                                                                      \
+  do {                                                                                             \
+    auto kern = k_ffx_rows_inv<DD, PP>;                                                            \
+    rc = set_dynamic_smem(kern, smem);                                                             \
+    if (rc == MRN_OK)                                                                              \
+      kern<<<blocks, nw * 32, smem, st>>>(P->d_slices, gsl, grow, fg.nsl, P->d_apod, P->d_grid, scale, \
+                                          out, fg.nrows, ax, P->d_ffx_tw);                         \
+  } while (0)
+    if (D == 2) { if (out) MRN_FFX_IROWS(2, true); else MRN_FFX_IROWS(2, false); }
+    else { if (out) MRN_FFX_IROWS(3, true); else MRN_FFX_IROWS(3, false); }
+#undef MRN_FFX_IROWS
+    if (rc != MRN_OK) return rc;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e);
+  }
+  return MRN_OK;
+}
+
+}  // namespace mrn

@@ -90,7 +90,26 @@ enum PostMode { kPostPlain = 0, kPostSense = 1 };
 int launch_post(mrn_plan* P, PostMode mode, const float2* mps, float2* out, float scale,
                 const float2* xin, float lam, double* pap, int pap_stride, cudaStream_t st);
 int launch_shift_copy(mrn_plan* P, const float2* src, float2* dst, int to_user, cudaStream_t st);
-int run_fft(mrn_plan* P, int direction, cudaStream_t st);
+// cuFFT of every FFT group, or (skip_native) of the groups the native passes
+// do not cover.
+int run_fft(mrn_plan* P, int direction, cudaStream_t st, bool skip_native = false);
+// Apodize / pad and forward FFT of the plan grid (native passes when
+// ffx_active, else k_pre + cuFFT), stage-timed; and the inverse FFT with the
+// plain crop / deapodize into out, or (out == nullptr) leaving the grid for a
+// SENSE post, which then reads only the lines that survive the crop.
+int fwd_transform(mrn_plan* P, PreMode mode, const float2* src, const float2* mps, float scale,
+                  cudaStream_t st);
+int inv_transform(mrn_plan* P, float2* out, cudaStream_t st);
+
+// Slice table upload (plan.cu): d_slices and its shared-k-space twin.
+cudaError_t upload_slices(mrn_plan* P);
+
+// Native FFT (ffx.cu)
+int ffx_setup(mrn_plan* P);
+int ffx_refresh(mrn_plan* P);  // slice flags after MRN_OPT_NATIVE_FFT changes
+bool ffx_active(const mrn_plan* P);
+int ffx_forward(mrn_plan* P, PreMode mode, const float2* src, const float2* mps, float scale, cudaStream_t st);
+int ffx_inverse(mrn_plan* P, float2* out, float scale, cudaStream_t st);
 
 // Toeplitz normal operator state (toeplitz.cu)
 void toep_free(mrn_plan* P);

@@ -102,8 +102,7 @@ extern "C" {
 int mrn_lr_forward(mrn_plan* P, const void* x, const void* mps, const void* w, void* ksp, void* s) {
   RK(check_lowrank(P));
   if (!x || !mps || !w || !ksp) return MRN_ERR_ARG;
-  { StageTimer t(P, kStagePre, ST(s)); RK(launch_pre(P, kPreSense, (const float2*)x, (const float2*)mps, 1.0f, ST(s))); }
-  { StageTimer t(P, kStageFft, ST(s)); RK(run_fft(P, CUFFT_FORWARD, ST(s))); }
+  RK(fwd_transform(P, kPreSense, (const float2*)x, (const float2*)mps, 1.0f, ST(s)));
   StageTimer t(P, kStageInterp, ST(s));
   RK(launch_interp(P, P->d_grid, kInternal, P->d_ksp_tmp, inv_width_prod(P), nullptr, ST(s)));
   return lr_combine(P, (const float2*)w, (float2*)ksp, ST(s));
@@ -114,7 +113,7 @@ int mrn_lr_adjoint(mrn_plan* P, const void* ksp, const void* w, const void* mps,
   RK(check_lowrank(P));
   if (!ksp || !w || !mps || !x) return MRN_ERR_ARG;
   { StageTimer t(P, kStageGrid, ST(s)); RK(lr_grid(P, (const float2*)ksp, (const float2*)w, ST(s))); }
-  { StageTimer t(P, kStageFft, ST(s)); RK(run_fft(P, CUFFT_INVERSE, ST(s))); }
+  RK(inv_transform(P, nullptr, ST(s)));
   StageTimer t(P, kStagePost, ST(s));
   return launch_post(P, kPostSense, (const float2*)mps, (float2*)x, out_scale, nullptr, 0.f, nullptr, 0,
                      ST(s));
@@ -124,8 +123,7 @@ int mrn_lr_normal(mrn_plan* P, const void* x, const void* mps, const void* w_fwd
                   void* out, float out_scale, float lam, void* s) {
   RK(check_lowrank(P));
   if (!x || !mps || !w_fwd || !w_adj || !out) return MRN_ERR_ARG;
-  { StageTimer t(P, kStagePre, ST(s)); RK(launch_pre(P, kPreSense, (const float2*)x, (const float2*)mps, 1.0f, ST(s))); }
-  { StageTimer t(P, kStageFft, ST(s)); RK(run_fft(P, CUFFT_FORWARD, ST(s))); }
+  RK(fwd_transform(P, kPreSense, (const float2*)x, (const float2*)mps, 1.0f, ST(s)));
   {
     // the combined samples overwrite component 0's block of the scratch
     StageTimer t(P, kStageInterp, ST(s));
@@ -133,7 +131,7 @@ int mrn_lr_normal(mrn_plan* P, const void* x, const void* mps, const void* w_fwd
     RK(lr_combine(P, (const float2*)w_fwd, P->d_ksp_tmp, ST(s)));
   }
   { StageTimer t(P, kStageGrid, ST(s)); RK(lr_grid(P, P->d_ksp_tmp, (const float2*)w_adj, ST(s))); }
-  { StageTimer t(P, kStageFft, ST(s)); RK(run_fft(P, CUFFT_INVERSE, ST(s))); }
+  RK(inv_transform(P, nullptr, ST(s)));
   StageTimer t(P, kStagePost, ST(s));
   return launch_post(P, kPostSense, (const float2*)mps, (float2*)out, out_scale, (const float2*)x, lam,
                      nullptr, 0, ST(s));

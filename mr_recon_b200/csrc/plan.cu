@@ -355,7 +355,7 @@ StageTimer::~StageTimer() {
 }
 
 // Upload the slice table and its shared-k-space twin (every ksp_off 0).
-static cudaError_t upload_slices(mrn_plan* P) {
+cudaError_t upload_slices(mrn_plan* P) {
   cudaError_t e = cudaMemcpy(P->d_slices, P->h_slices.data(), P->nslices * sizeof(SliceGeom),
                              cudaMemcpyHostToDevice);
   if (e != cudaSuccess || !P->d_slices_kshared) return e;
@@ -691,6 +691,7 @@ int mrn_plan_create(mrn_plan** out, int ndim, int n_slices, const int* im_size,
                                     fg.batch);
       if (r != CUFFT_SUCCESS) { fg.handle = 0; mrn_plan_destroy(P); return MRN_ERR_CUFFT; }
     }
+    PK(ffx_setup(P));
   }
 #undef PK
   *out = P;
@@ -720,6 +721,9 @@ int mrn_plan_set_option(mrn_plan* P, int option, int value) {
       P->use_ent = value != 0;
       P->traj_set = false;  // the entry map is built (or not) at mrn_plan_set_traj
       return MRN_OK;
+    case MRN_OPT_NATIVE_FFT:
+      P->use_ffx = value != 0;
+      return ffx_refresh(P);
     case MRN_OPT_GRID_LANES:
       if (value != 0 && value != 8 && value != 16 && value != 32) return MRN_ERR_ARG;
       P->grid_lanes = value;
@@ -779,7 +783,7 @@ int mrn_plan_destroy(mrn_plan* P) {
                   P->d_ksp_tmp, P->d_sync, P->d_wmeta_i, P->d_wtab_i, P->d_wmeta_g,
                   P->d_wtab_g, P->d_part, P->d_items_tmp, P->d_sort_key[0], P->d_sort_key[1],
                   P->d_sort_idx[0], P->d_sort_idx[1], P->d_red, P->d_rowpart, P->d_ent_of,
-                  P->d_ksp_ent};
+                  P->d_ksp_ent, P->d_ffx_tw, P->d_ffx_sl, P->d_ffx_row};
   for (void* b : bufs)
     if (b) cudaFree(b);
   delete P;
