@@ -100,6 +100,7 @@ struct FfxAxis {
   int ns;
   int radix[kFfxMaxStages];
   int tw_off[kFfxMaxStages];
+  unsigned magic[kFfxMaxStages];  // floor(2^32 / L) + 1: b / L = umulhi(b, magic) for b, L <= kFfxMaxN
   int tw_base;  // first entry of this axis in the plan's twiddle table
 };
 

@@ -97,33 +97,26 @@ __device__ __forceinline__ void dft(float2 (&x)[R]) {
   }
 }
 
-// Butterfly bi of a stage (radix R, L, n / R = nr) over elements es apart.
-template <int R, bool INV>
-__device__ __forceinline__ void bfly(const float2* __restrict__ a, float2* __restrict__ b, int L, int nr,
-                                     const float2* __restrict__ tw, int bi, int es) {
-  const int k = bi / L, j = bi - k * L;
+// Butterfly bi of a stage (radix R, L, nr = n / R) over elements ES apart;
+// k = bi / L by a multiply-high with the stage's magic (the first stage has
+// L = 1 and no twiddles).
+template <int R, bool INV, int ES, bool FIRST>
+__device__ __forceinline__ void bfly(const float2* __restrict__ a, float2* __restrict__ b, int L, unsigned magic,
+                                     int nr, const float2* __restrict__ tw, int bi) {
+  const int k = FIRST ? bi : (int)__umulhi((unsigned)bi, magic);
+  const int j = FIRST ? 0 : bi - k * L;
   float2 x[R];
 #pragma unroll
-  for (int t = 0; t < R; ++t) x[t] = a[(bi + t * nr) * es];
-  if (j > 0) {
+  for (int t = 0; t < R; ++t) x[t] = a[(bi + t * nr) * ES];
+  if (!FIRST) {
+    const float2* tj = tw + j * (R - 1);
 #pragma unroll
-    for (int t = 1; t < R; ++t) x[t] = ctw<INV>(x[t], tw[j * (R - 1) + t - 1]);
+    for (int t = 1; t < R; ++t) x[t] = ctw<INV>(x[t], tj[t - 1]);
   }
   dft<R, INV>(x);
   const int ob = k * R * L + j;
 #pragma unroll
-  for (int u = 0; u < R; ++u) b[(ob + u * L) * es] = x[u];
-}
-
-template <bool INV>
-__device__ __forceinline__ void bfly_any(int R, const float2* a, float2* b, int L, int nr, const float2* tw,
-                                         int bi, int es) {
-  switch (R) {
-    case 4: bfly<4, INV>(a, b, L, nr, tw, bi, es); break;
-    case 5: bfly<5, INV>(a, b, L, nr, tw, bi, es); break;
-    case 3: bfly<3, INV>(a, b, L, nr, tw, bi, es); break;
-    default: bfly<2, INV>(a, b, L, nr, tw, bi, es); break;
-  }
+  for (int u = 0; u < R; ++u) b[(ob + u * L) * ES] = x[u];
 }
 
 // Axis plan in shared memory (kernel parameters indexed at run time would go
@@ -131,6 +124,7 @@ __device__ __forceinline__ void bfly_any(int R, const float2* a, float2* b, int 
 struct FfxShared {
   int radix[kFfxMaxStages];
   int tw_off[kFfxMaxStages];
+  unsigned magic[kFfxMaxStages];
 };
 
 __device__ __forceinline__ void stage_axis(FfxShared& sa, float2* tw, const FfxAxis& ax,
@@ -140,10 +134,47 @@ __device__ __forceinline__ void stage_axis(FfxShared& sa, float2* tw, const FfxA
     for (int i = 0; i < kFfxMaxStages; ++i) {
       sa.radix[i] = ax.radix[i];
       sa.tw_off[i] = ax.tw_off[i];
+      sa.magic[i] = ax.magic[i];
     }
   }
   for (int i = threadIdx.x; i < ax.n - 1; i += blockDim.x) tw[i] = twg[ax.tw_base + i];
 }
+
+// All butterflies of one stage of a line (ES = 1) by the lanes of a warp.
+template <int R, bool INV, bool FIRST>
+__device__ __forceinline__ void line_stage(const float2* a, float2* b, int L, unsigned magic, int nr,
+                                           const float2* tw, int lane) {
+  for (int bi = lane; bi < nr; bi += 32) bfly<R, INV, 1, FIRST>(a, b, L, magic, nr, tw, bi);
+}
+
+// One stage over W adjacent columns (elements W apart) by a CTA.
+template <int R, bool INV, bool FIRST, int W>
+__device__ __forceinline__ void cols_stage(const float2* a, float2* b, int L, unsigned magic, int nr,
+                                           const float2* tw, int tid, int nt) {
+  for (int idx = tid; idx < nr * W; idx += nt) {
+    const int bi = idx / W, w = idx - bi * W;
+    bfly<R, INV, W, FIRST>(a + w, b + w, L, magic, nr, tw, bi);
+  }
+}
+
+#define MRN_FFX_STAGE(CALL)                                  \
+  do {                                                       \
+    if (s == 0) {                                            \
+      switch (R) {                                           \
+        case 4: CALL(4, true); break;                        \
+        case 5: CALL(5, true); break;                        \
+        case 3: CALL(3, true); break;                        \
+        default: CALL(2, true); break;                       \
+      }                                                      \
+    } else {                                                 \
+      switch (R) {                                           \
+        case 4: CALL(4, false); break;                       \
+        case 5: CALL(5, false); break;                       \
+        case 3: CALL(3, false); break;                       \
+        default: CALL(2, false); break;                      \
+      }                                                      \
+    }                                                        \
+  } while (0)
 
 // One line of n points by one warp: a holds the input, b is scratch; returns
 // the buffer that holds the transform.
@@ -153,8 +184,11 @@ __device__ __forceinline__ float2* line_fft(float2* a, float2* b, int n, int ns,
   int L = 1;
   for (int s = 0; s < ns; ++s) {
     const int R = sa.radix[s], nr = n / R;
+    const unsigned magic = sa.magic[s];
     const float2* t = tw + sa.tw_off[s];
-    for (int bi = lane; bi < nr; bi += 32) bfly_any<INV>(R, a, b, L, nr, t, bi, 1);
+#define MRN_LINE_CALL(RR, FF) line_stage<RR, INV, FF>(a, b, L, magic, nr, t, lane)
+    MRN_FFX_STAGE(MRN_LINE_CALL);
+#undef MRN_LINE_CALL
     __syncwarp();
     float2* tmp = a;
     a = b;
@@ -350,11 +384,11 @@ k_ffx_cols(float2* __restrict__ grid, FfxAxis ax, const float2* __restrict__ twg
   int L = 1;
   for (int s = 0; s < ax.ns; ++s) {
     const int R = sa.radix[s], nr = n / R;
+    const unsigned magic = sa.magic[s];
     const float2* t = tw + sa.tw_off[s];
-    for (int idx = tid; idx < nr * W; idx += kFfxThreads) {
-      const int bi = idx / W, w = idx - bi * W;
-      bfly_any<INV>(R, A + w, B + w, L, nr, t, bi, W);
-    }
+#define MRN_COLS_CALL(RR, FF) cols_stage<RR, INV, FF, W>(A, B, L, magic, nr, t, tid, kFfxThreads)
+    MRN_FFX_STAGE(MRN_COLS_CALL);
+#undef MRN_COLS_CALL
     __syncthreads();
     float2* tmp = A;
     A = B;
@@ -500,6 +534,7 @@ int ffx_setup(mrn_plan* P) {
       for (int s = 0; s < ax.ns; ++s) {
         const int R = ax.radix[s];
         ax.tw_off[s] = off;
+        ax.magic[s] = L > 1 ? (unsigned)((1ull << 32) / (unsigned long long)L + 1ull) : 0u;
         for (int j = 0; j < L; ++j)
           for (int t = 1; t < R; ++t) {
             const double ang = -2.0 * M_PI * (double)t * (double)j / (double)(L * R);
