@@ -263,13 +263,18 @@ k_ffx_rows_fwd(const SliceGeom* __restrict__ sl, const int* __restrict__ gsl, co
   const float2* mrow = SENSE ? mps + g.img_off + (int64_t)c * g.nimg + qlin : nullptr;
   float2* A = fsm + n + warp * 2 * n;
   float2* B = A + n;
-#pragma unroll 4
+  // the image row lands in B (the FFT's scratch) with every copy in flight
+  // at once, then is apodized and placed into A
+  for (int q = lane; q < nl; q += 32) cp_async8(&B[q], srow + q);
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncwarp();
   for (int j = lane; j < n; j += 32) {
     int q = j + h;
     if (q >= n) q -= n;
     float2 v = make_float2(0.f, 0.f);
     if (q < nl) {
-      float2 x = __ldg(srow + q);
+      float2 x = B[q];
       if (SENSE) {
         const float2 m = __ldg(mrow + q);
         x = make_float2(x.x * m.x - x.y * m.y, x.x * m.y + x.y * m.x);
@@ -328,8 +333,9 @@ k_ffx_rows_inv(const SliceGeom* __restrict__ sl, const int* __restrict__ gsl, co
   float2* gline = grid + g.grid_off + (int64_t)c * g.gos + lrow * n;
   float2* A = fsm + n + warp * 2 * n;
   float2* B = A + n;
-#pragma unroll 4
-  for (int j = lane; j < n; j += 32) A[j] = gline[j];
+  for (int j = lane; j < n; j += 32) cp_async8(&A[j], gline + j);
+  cp_async_commit();
+  cp_async_wait<0>();
   __syncwarp();
   const float2* res = line_fft<true>(A, B, n, ax.ns, sa, tw, lane);
   if (!POST) {
@@ -407,7 +413,8 @@ int rows_warps(int n) {
   return std::max(1, std::min(8, w));
 }
 
-int launch_cols(mrn_plan* P, int q, int a, bool inv, cudaStream_t st) {
+template <int W>
+int launch_cols_w(mrn_plan* P, int q, int a, bool inv, cudaStream_t st) {
   const int D = P->ndim;
   const mrn_plan::FfxGroup& fg = P->ffx[q];
   const SliceGeom& g = P->h_slices[fg.first_slice];
@@ -415,7 +422,6 @@ int launch_cols(mrn_plan* P, int q, int a, bool inv, cudaStream_t st) {
   int64_t stride = 1, outer = P->fft[q].batch;
   for (int i = a + 1; i < D; ++i) stride *= g.nos[i];
   for (int i = 0; i < a; ++i) outer *= g.nos[i];
-  constexpr int W = kFfxCols;
   const int64_t nib = (stride + W - 1) / W;
   const int64_t nblocks = outer * nib;
   if (nblocks <= 0) return MRN_OK;
@@ -438,6 +444,16 @@ int launch_cols(mrn_plan* P, int q, int a, bool inv, cudaStream_t st) {
   if (rc != MRN_OK) return rc;
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? MRN_OK : cuda_fail(e);
+}
+
+// 3D grids (the passes stream from HBM) take blocks of 16 columns (128-byte
+// row segments) while those fit in 100 KB of shared memory; 2D grids, which
+// stay in L2, take 8 (more CTAs per SM).
+int launch_cols(mrn_plan* P, int q, int a, bool inv, cudaStream_t st) {
+  const int n = P->ffx[q].ax[a].n;
+  if (P->ndim == 3 && ((size_t)n + 32 * (size_t)n) * sizeof(float2) <= 100 * 1024)
+    return launch_cols_w<16>(P, q, a, inv, st);
+  return launch_cols_w<kFfxCols>(P, q, a, inv, st);
 }
 
 // Radices for n (4 first, then 5, 3, 2); false if n has another prime factor.
