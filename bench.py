@@ -712,6 +712,7 @@ def main():
     torch.cuda.synchronize()
     plan = nf._plans.entries[-1][2]
     stats = plan.stats()
+    stats["fft_kind"] = plan.fft_kind
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
 
     def step():
@@ -980,7 +981,10 @@ def main():
         if "c5" in want:
             extra["c5"] = bench_c5(dev)
 
-    launches_per_step = 4 + (1 if stats["split_tiles"] > 0 else 0)
+    # own kernels per fwd+adj step: interpolation and gridding, plus either the
+    # four native FFT passes (pad and crop fused) or k_pre / k_post around cuFFT,
+    # plus the split-tile reduction
+    launches_per_step = 2 + (4 if stats["fft_kind"] == 1 else 2) + (1 if stats["split_tiles"] > 0 else 0)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

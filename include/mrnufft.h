@@ -85,6 +85,12 @@ int mrn_plan_sizes(const mrn_plan* plan, int64_t* out8);
  * before mrn_plan_set_traj). Synchronises the plan's device to read them. */
 int mrn_plan_stats(mrn_plan* plan, int64_t* out4);
 
+/* Which FFT the plan's transforms run (no counterpart in the reference):
+ * 0 cuFFT for every grid size, 1 the native per-axis passes for every grid
+ * size (MRN_OPT_NATIVE_FFT), 2 native for some FFT groups and cuFFT for the
+ * others; a negative MRN_ERR_* code for a null plan. */
+int mrn_plan_fft_kind(const mrn_plan* plan);
+
 /* Plan options (no counterpart in the reference).
  * MRN_OPT_FAST_KERNELS (default 1): use the unrolled fixed-width tile kernels
  * where they apply (2D/3D, equal width in [4, 8) per dimension); 0 forces the

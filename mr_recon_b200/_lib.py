@@ -59,6 +59,7 @@ SIGNATURES = {
     "mrn_plan_offsets": (_i, [_vp, _pi64, _pi64, _pi64, _pi64]),
     "mrn_plan_sizes": (_i, [_vp, _pi64]),
     "mrn_plan_stats": (_i, [_vp, _pi64]),
+    "mrn_plan_fft_kind": (_i, [_vp]),
     "mrn_plan_set_option": (_i, [_vp, _i, _i]),
     "mrn_plan_set_beta": (_i, [_vp, _pd]),
     "mrn_plan_enable_timing": (_i, [_vp, _i]),

@@ -810,6 +810,12 @@ int mrn_plan_sizes(const mrn_plan* P, int64_t* o) {
   return MRN_OK;
 }
 
+int mrn_plan_fft_kind(const mrn_plan* P) {
+  if (!P) return MRN_ERR_ARG;
+  if (!ffx_active(P)) return 0;
+  return P->ffx_all ? 1 : 2;
+}
+
 int mrn_plan_stats(mrn_plan* P, int64_t* o) {
   if (!P || !o) return MRN_ERR_ARG;
   int hc[4] = {0, 0, 0, 0};

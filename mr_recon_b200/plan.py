@@ -112,6 +112,14 @@ class Plan:
         check(self.lib.mrn_plan_stats(self.handle, o))
         return {"interp_items": o[0], "grid_items": o[1], "grid_entries": o[2], "split_tiles": o[3]}
 
+    @property
+    def fft_kind(self) -> int:
+        """mrn_plan_fft_kind: 0 cuFFT, 1 the native per-axis FFT passes for
+        every grid size, 2 native for some grid sizes only."""
+        r = self.lib.mrn_plan_fft_kind(self.handle)
+        check(min(r, 0))
+        return r
+
     def set_option(self, option: int, value: int) -> None:
         """mrn_plan_set_option. Chunk and tile options take effect at the next
         set_traj (the trajectory is unbound until then)."""

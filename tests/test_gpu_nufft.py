@@ -420,6 +420,7 @@ def test_uneven_multislice_plan_matches_per_slice_oracle():
     coils = [3, 1, 5, 2]
     npts = [900, 400, 1300, 700]
     plan = Plan(sizes, npts, coils, 1.25, (6.0, 6.0), device=DEV)
+    assert plan.fft_kind == 2  # 50 and 60 x 40 natively, 70 (= 2 x 5 x 7) on cuFFT
     trjs = [((rng.rand(m, 2) - 0.5) * np.array(s)).astype(np.float32) for s, m in zip(sizes, npts)]
     imgs = [synth.randn_complex((c, *s), rng) for s, c in zip(sizes, coils)]
     plan.set_traj(T(np.concatenate([t.reshape(-1) for t in trjs])))
@@ -826,6 +827,7 @@ def test_native_fft_matches_cufft_and_oracle(im, os_, native):
         p = Plan([im], [M], [C], os_, (float(W),) * d, device=DEV)
         p.set_option(_lib.MRN_OPT_NATIVE_FFT, opt)
         p.set_traj(T(trj))
+        assert p.fft_kind == (1 if (opt and native) else 0)
         ksp = torch.empty(C * M, dtype=torch.complex64, device=DEV)
         out = torch.empty(C * nimg, dtype=torch.complex64, device=DEV)
         p.forward(T(img).reshape(-1), ksp)
