@@ -104,6 +104,42 @@ struct FfxAxis {
   int tw_base;  // first entry of this axis in the plan's twiddle table
 };
 
+// One FFT group of a grid buffer (slices of one grid size, back to back as
+// [batch][nos...]). native: its slices have the same image size and every
+// axis factors into radices 2-5 with at most kFfxMaxN points.
+struct FfxGroup {
+  bool native;
+  FfxAxis ax[kMaxDim];
+  int first_slice;  // geometry (image and grid size) shared by the group's slices
+  int nsl;          // slices in the group
+  int sl_off;       // their ids at FfxSet::d_sl + sl_off, in grid order
+  int row_off;      // first grid row of each at FfxSet::d_row + row_off (nsl + 1 entries)
+  int64_t nrows;    // grid rows (coils x all axes but the last) of the group
+  int64_t grid_off; // complex offset of the group's block in its grid buffer
+  int batch;        // coils of the group
+};
+
+// The native FFT of one grid buffer: its groups, their twiddle tables and
+// slice / row lists (host side owns the device arrays; release() frees them).
+struct FfxSet {
+  bool ok = false;   // some group is native
+  bool all = false;  // every group is native
+  std::vector<FfxGroup> grp;
+  float2* d_tw = nullptr;
+  int* d_sl = nullptr;
+  int64_t* d_row = nullptr;
+  void release() {
+    if (d_tw) cudaFree(d_tw);
+    if (d_sl) cudaFree(d_sl);
+    if (d_row) cudaFree(d_row);
+    d_tw = nullptr;
+    d_sl = nullptr;
+    d_row = nullptr;
+    grp.clear();
+    ok = all = false;
+  }
+};
+
 struct KBParams {
   float radius[kMaxDim];  // W_i / 2
   float beta;             // beta of dimension 0 (all dimensions when uniform_beta)
@@ -430,26 +466,10 @@ struct mrn_plan {
     cufftHandle handle;
   };
   std::vector<FftGroup> fft;
-  // Native FFT (ffx.cu), per FFT group: used for a group whose slices have
-  // the same image size and whose grid axes factor into radices 2-5 with at
-  // most kFfxMaxN points; other groups keep cuFFT. MRN_OPT_NATIVE_FFT
+  // Native FFT (ffx.cu) of the plan grid's FFT groups; MRN_OPT_NATIVE_FFT
   // selects it (default) or cuFFT for every group.
-  struct FfxGroup {
-    bool native;      // the group's axes and slices qualify
-    mrn::FfxAxis ax[mrn::kMaxDim];
-    int first_slice;  // geometry (image and grid size) shared by the group's slices
-    int nsl;          // slices in the group
-    int sl_off;       // their ids at d_ffx_sl + sl_off, in grid order
-    int row_off;      // first grid row of each at d_ffx_row + row_off (nsl + 1 entries)
-    int64_t nrows;    // grid rows (coils x all axes but the last) of the group
-  };
-  bool ffx_ok = false;   // some group is native
-  bool ffx_all = false;  // every group is native
+  mrn::FfxSet ffx;
   bool use_ffx = true;
-  std::vector<FfxGroup> ffx;
-  float2* d_ffx_tw = nullptr;   // twiddle tables of every group's axes, back to back
-  int* d_ffx_sl = nullptr;
-  int64_t* d_ffx_row = nullptr;
 
   // Optional stage timing (mrn_plan_enable_timing): CUDA event pairs recorded
   // on the launching stream around each stage, summed by mrn_plan_timing.

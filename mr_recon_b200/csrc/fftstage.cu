@@ -373,7 +373,7 @@ int fwd_transform(mrn_plan* P, PreMode mode, const float2* src, const float2* mp
                   cudaStream_t st) {
   if (ffx_active(P)) {
     StageTimer t(P, kStageFft, st);
-    if (!P->ffx_all) {  // groups left to cuFFT: pad them (k_pre skips native slices) and transform
+    if (!P->ffx.all) {  // groups left to cuFFT: pad them (k_pre skips native slices) and transform
       int rc = launch_pre(P, mode, src, mps, scale, st);
       if (rc == MRN_OK) rc = run_fft(P, CUFFT_FORWARD, st, true);
       if (rc != MRN_OK) return rc;
@@ -393,7 +393,7 @@ int inv_transform(mrn_plan* P, float2* out, cudaStream_t st) {
   if (ffx_active(P)) {
     StageTimer t(P, kStageFft, st);
     int rc = ffx_inverse(P, out, 1.0f, st);
-    if (rc != MRN_OK || P->ffx_all) return rc;
+    if (rc != MRN_OK || P->ffx.all) return rc;
     rc = run_fft(P, CUFFT_INVERSE, st, true);  // k_post then skips native slices
     if (rc != MRN_OK || !out) return rc;
     return launch_post(P, kPostPlain, nullptr, out, 1.0f, nullptr, 0.f, nullptr, 0, st);
@@ -411,7 +411,7 @@ int inv_transform(mrn_plan* P, float2* out, cudaStream_t st) {
 int run_fft(mrn_plan* P, int direction, cudaStream_t st, bool skip_native) {
   for (size_t q = 0; q < P->fft.size(); ++q) {
     auto& fg = P->fft[q];
-    if (skip_native && q < P->ffx.size() && P->ffx[q].native) continue;
+    if (skip_native && q < P->ffx.grp.size() && P->ffx.grp[q].native) continue;
     if (cufftSetStream(fg.handle, st) != CUFFT_SUCCESS) return MRN_ERR_CUFFT;
     cufftComplex* p = reinterpret_cast<cufftComplex*>(P->d_grid + fg.grid_off);
     if (cufftExecC2C(fg.handle, p, p, direction) != CUFFT_SUCCESS) return MRN_ERR_CUFFT;

@@ -356,6 +356,43 @@ k_ffx_rows_inv(const SliceGeom* __restrict__ sl, const int* __restrict__ gsl, co
   }
 }
 
+// All stages of a column block's FFT (W columns, elements W apart) by a CTA;
+// on return A holds the transform (B is scratch).
+template <bool INV, int W>
+__device__ __forceinline__ void cols_fft(float2*& A, float2*& B, int n, int ns, const FfxShared& sa,
+                                         const float2* tw, int tid) {
+  int L = 1;
+  for (int s = 0; s < ns; ++s) {
+    const int R = sa.radix[s], nr = n / R;
+    const unsigned magic = sa.magic[s];
+    const float2* t = tw + sa.tw_off[s];
+#define MRN_COLS_CALL(RR, FF) cols_stage<RR, INV, FF, W>(A, B, L, magic, nr, t, tid, kFfxThreads)
+    MRN_FFX_STAGE(MRN_COLS_CALL);
+#undef MRN_COLS_CALL
+    __syncthreads();
+    float2* tmp = A;
+    A = B;
+    B = tmp;
+    L *= R;
+  }
+}
+
+// Copy a column block [n][W] into shared memory (cp.async); rows outside
+// `keep` (zero padding of the axis, when masked) and columns past the end
+// read as zero.
+template <int W>
+__device__ __forceinline__ void cols_load(float2* A, const float2* base, int64_t stride, int wn, int n, int n_img,
+                                          bool mask, int tid) {
+  for (int idx = tid; idx < n * W; idx += kFfxThreads) {
+    const int rr = idx / W, w = idx - rr * W;
+    if (w < wn && (!mask || kept(rr, n_img, n))) cp_async8(&A[idx], base + rr * stride + w);
+    else A[idx] = make_float2(0.f, 0.f);
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+}
+
 // One strided axis: the grid as [outer][n][stride] (stride = product of the
 // later axes' sizes), a CTA per (outer index, block of W adjacent columns).
 // Forward: rows in the axis' zero padding read as zero; inverse: only rows
@@ -379,28 +416,8 @@ k_ffx_cols(float2* __restrict__ grid, FfxAxis ax, const float2* __restrict__ twg
   const int64_t w0 = ib * W;
   const int wn = (int)min((int64_t)W, stride - w0);
   float2* base = grid + o * n * stride + w0;
-  for (int idx = tid; idx < n * W; idx += kFfxThreads) {
-    const int rr = idx / W, w = idx - rr * W;
-    if (w < wn && (INV || kept(rr, n_img, n))) cp_async8(&A[idx], base + rr * stride + w);
-    else A[idx] = make_float2(0.f, 0.f);
-  }
-  cp_async_commit();
-  cp_async_wait<0>();
-  __syncthreads();
-  int L = 1;
-  for (int s = 0; s < ax.ns; ++s) {
-    const int R = sa.radix[s], nr = n / R;
-    const unsigned magic = sa.magic[s];
-    const float2* t = tw + sa.tw_off[s];
-#define MRN_COLS_CALL(RR, FF) cols_stage<RR, INV, FF, W>(A, B, L, magic, nr, t, tid, kFfxThreads)
-    MRN_FFX_STAGE(MRN_COLS_CALL);
-#undef MRN_COLS_CALL
-    __syncthreads();
-    float2* tmp = A;
-    A = B;
-    B = tmp;
-    L *= R;
-  }
+  cols_load<W>(A, base, stride, wn, n, n_img, !INV, tid);
+  cols_fft<INV, W>(A, B, n, ax.ns, sa, tw, tid);
   for (int idx = tid; idx < n * W; idx += kFfxThreads) {
     const int rr = idx / W, w = idx - rr * W;
     if (w < wn && (!INV || kept(rr, n_img, n))) base[rr * stride + w] = A[idx];
@@ -413,13 +430,14 @@ int rows_warps(int n) {
   return std::max(1, std::min(8, w));
 }
 
+// One strided pass of group q along axis a.
 template <int W>
-int launch_cols_w(mrn_plan* P, int q, int a, bool inv, cudaStream_t st) {
-  const int D = P->ndim;
-  const mrn_plan::FfxGroup& fg = P->ffx[q];
-  const SliceGeom& g = P->h_slices[fg.first_slice];
+int launch_cols_w(const FfxSet& S, const FfxGrid& G, int q, int a, bool inv, cudaStream_t st) {
+  const int D = G.ndim;
+  const FfxGroup& fg = S.grp[q];
+  const SliceGeom& g = G.hsl[fg.first_slice];
   const FfxAxis& ax = fg.ax[a];
-  int64_t stride = 1, outer = P->fft[q].batch;
+  int64_t stride = 1, outer = fg.batch;
   for (int i = a + 1; i < D; ++i) stride *= g.nos[i];
   for (int i = 0; i < a; ++i) outer *= g.nos[i];
   const int64_t nib = (stride + W - 1) / W;
@@ -428,18 +446,19 @@ int launch_cols_w(mrn_plan* P, int q, int a, bool inv, cudaStream_t st) {
   if (nblocks > 0x7fffffffLL) return MRN_ERR_UNSUPPORTED;
   const size_t smem = ((size_t)ax.n + 2 * (size_t)ax.n * W) * sizeof(float2);
   const int skip_n = a == 1 ? g.n[0] : 0, skip_nos = a == 1 ? g.nos[0] : 0;
-  float2* grid = P->d_grid + P->fft[q].grid_off;
+  float2* grid = G.grid + fg.grid_off;
+  const unsigned nb = (unsigned)nblocks;
   int rc;
   if (inv) {
-    auto kern = k_ffx_cols<true, W>;
-    rc = set_dynamic_smem(kern, smem);
+    auto kernf = k_ffx_cols<true, W>;
+    rc = set_dynamic_smem(kernf, smem);
     if (rc == MRN_OK)
-      kern<<<(unsigned)nblocks, kFfxThreads, smem, st>>>(grid, ax, P->d_ffx_tw, stride, nib, g.n[a], skip_n, skip_nos);
+      kernf<<<nb, kFfxThreads, smem, st>>>(grid, ax, S.d_tw, stride, nib, g.n[a], skip_n, skip_nos);
   } else {
-    auto kern = k_ffx_cols<false, W>;
-    rc = set_dynamic_smem(kern, smem);
+    auto kernf = k_ffx_cols<false, W>;
+    rc = set_dynamic_smem(kernf, smem);
     if (rc == MRN_OK)
-      kern<<<(unsigned)nblocks, kFfxThreads, smem, st>>>(grid, ax, P->d_ffx_tw, stride, nib, g.n[a], skip_n, skip_nos);
+      kernf<<<nb, kFfxThreads, smem, st>>>(grid, ax, S.d_tw, stride, nib, g.n[a], skip_n, skip_nos);
   }
   if (rc != MRN_OK) return rc;
   cudaError_t e = cudaGetLastError();
@@ -449,11 +468,56 @@ int launch_cols_w(mrn_plan* P, int q, int a, bool inv, cudaStream_t st) {
 // 3D grids (the passes stream from HBM) take blocks of 16 columns (128-byte
 // row segments) while those fit in 100 KB of shared memory; 2D grids, which
 // stay in L2, take 8 (more CTAs per SM).
-int launch_cols(mrn_plan* P, int q, int a, bool inv, cudaStream_t st) {
-  const int n = P->ffx[q].ax[a].n;
-  if (P->ndim == 3 && ((size_t)n + 32 * (size_t)n) * sizeof(float2) <= 100 * 1024)
-    return launch_cols_w<16>(P, q, a, inv, st);
-  return launch_cols_w<kFfxCols>(P, q, a, inv, st);
+int launch_cols(const FfxSet& S, const FfxGrid& G, int q, int a, bool inv, cudaStream_t st) {
+  const int n = S.grp[q].ax[a].n;
+  if (G.ndim == 3 && ((size_t)n + 32 * (size_t)n) * sizeof(float2) <= 100 * 1024)
+    return launch_cols_w<16>(S, G, q, a, inv, st);
+  return launch_cols_w<kFfxCols>(S, G, q, a, inv, st);
+}
+
+// Last-axis pass of group q: forward fused with the pad (mode), or inverse
+// with the crop into out (out != nullptr) or stored back in place.
+int launch_rows(const FfxSet& S, const FfxGrid& G, int q, bool inv, PreMode mode, const float2* src,
+                const float2* mps, float2* out, float scale, cudaStream_t st) {
+  const int D = G.ndim;
+  const FfxGroup& fg = S.grp[q];
+  const FfxAxis& ax = fg.ax[D - 1];
+  const int nw = rows_warps(ax.n);
+  const unsigned blocks = (unsigned)((fg.nrows + nw - 1) / nw);
+  if (blocks == 0) return MRN_OK;
+  const size_t smem = ((size_t)ax.n + 2 * (size_t)nw * ax.n) * sizeof(float2);
+  const int* gsl = S.d_sl + fg.sl_off;
+  const int64_t* grow = S.d_row + fg.row_off;
+  const bool sense = mode == kPreSense;
+  int rc = MRN_OK;
+#define MRN_FFX_ROWS(DD, SS)                                                                       \
+  do {                                                                                             \
+    auto kern = k_ffx_rows_fwd<DD, SS>;                                                            \
+    rc = set_dynamic_smem(kern, smem);                                                             \
+    if (rc == MRN_OK)                                                                              \
+      kern<<<blocks, nw * 32, smem, st>>>(G.dsl, gsl, grow, fg.nsl, G.apod, src, mps, scale, G.grid, \
+                                          fg.nrows, ax, S.d_tw);                                   \
+  } while (0)
+#define MRN_FFX_IROWS(DD, PP)                                                                      \
+  do {                                                                                             \
+    auto kern = k_ffx_rows_inv<DD, PP>;                                                            \
+    rc = set_dynamic_smem(kern, smem);                                                             \
+    if (rc == MRN_OK)                                                                              \
+      kern<<<blocks, nw * 32, smem, st>>>(G.dsl, gsl, grow, fg.nsl, G.apod, G.grid, scale, out,   \
+                                          fg.nrows, ax, S.d_tw);                                   \
+  } while (0)
+  if (!inv) {
+    if (D == 2) { if (sense) MRN_FFX_ROWS(2, true); else MRN_FFX_ROWS(2, false); }
+    else { if (sense) MRN_FFX_ROWS(3, true); else MRN_FFX_ROWS(3, false); }
+  } else {
+    if (D == 2) { if (out) MRN_FFX_IROWS(2, true); else MRN_FFX_IROWS(2, false); }
+    else { if (out) MRN_FFX_IROWS(3, true); else MRN_FFX_IROWS(3, false); }
+  }
+#undef MRN_FFX_ROWS
+#undef MRN_FFX_IROWS
+  if (rc != MRN_OK) return rc;
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? MRN_OK : cuda_fail(e);
 }
 
 // Radices for n (4 first, then 5, 3, 2); false if n has another prime factor.
@@ -483,54 +547,41 @@ int upload(T** dst, const std::vector<T>& v) {
   return MRN_OK;
 }
 
-}  // namespace
-
-bool ffx_active(const mrn_plan* P) { return P->ffx_ok && P->use_ffx; }
-
-// Per-slice flags: the slice's group runs the native passes (and k_pre /
-// k_post leave it alone).
-int ffx_refresh(mrn_plan* P) {
-  if (P->h_slices.empty() || !P->d_slices) return MRN_OK;
-  const int D = P->ndim;
-  for (auto& g : P->h_slices) {
-    g.native_fft = 0;
-    if (!P->use_ffx) continue;
-    for (const auto& fg : P->ffx) {
-      bool same = fg.native;
-      for (int i = 0; i < D && same; ++i) same = g.nos[i] == fg.ax[i].n;
-      if (same) g.native_fft = 1;
-    }
-  }
-  return upload_slices(P) == cudaSuccess ? MRN_OK : MRN_ERR_CUDA;
+FfxGrid plan_grid(mrn_plan* P) {
+  return FfxGrid{P->ndim, P->h_slices.data(), P->d_slices, P->d_apod, P->d_grid};
 }
 
-// Decide, per FFT group, whether the native FFT applies and build its axes'
-// twiddle tables and its slice / row lists (plan creation, after the FFT
-// groups exist). A group whose slices differ in image size, or with an axis
-// that has a prime factor above 5 or more than kFfxMaxN points, keeps cuFFT.
-int ffx_setup(mrn_plan* P) {
-  P->ffx_ok = P->ffx_all = false;
-  P->ffx.clear();
-  if ((P->flags & MRN_PLAN_RAW) || (P->ndim != 2 && P->ndim != 3) || P->h_slices.empty()) return MRN_OK;
-  const int D = P->ndim;
+}  // namespace
+
+// Build the native FFT of a grid buffer: per group spec (grid size, block
+// offset, coils), the group's slices (those of that grid size, in slice
+// order), its axes' twiddle tables and slice / row lists. A group whose
+// slices differ in image size, or with an axis that has a prime factor above
+// 5 or more than kFfxMaxN points, is not native.
+int ffx_build(FfxSet& S, int ndim, const std::vector<SliceGeom>& hsl, const std::vector<FfxGroupSpec>& spec) {
+  S.release();
+  if ((ndim != 2 && ndim != 3) || hsl.empty()) return MRN_OK;
+  const int D = ndim;
   std::vector<float2> tab;
   std::vector<int> sl_ids;
   std::vector<int64_t> rows;
   int nnative = 0;
-  for (size_t q = 0; q < P->fft.size(); ++q) {
-    mrn_plan::FfxGroup fg{};
+  for (const FfxGroupSpec& gs : spec) {
+    FfxGroup fg{};
     fg.native = true;
     fg.first_slice = -1;
     fg.sl_off = (int)sl_ids.size();
     fg.row_off = (int)rows.size();
+    fg.grid_off = gs.grid_off;
+    fg.batch = gs.batch;
     int64_t r = 0;
-    for (int s = 0; s < (int)P->h_slices.size(); ++s) {
-      const SliceGeom& g = P->h_slices[s];
+    for (int s = 0; s < (int)hsl.size(); ++s) {
+      const SliceGeom& g = hsl[s];
       bool same = true;
-      for (int i = 0; i < D; ++i) same &= g.nos[i] == P->fft[q].nos[i];
+      for (int i = 0; i < D; ++i) same &= g.nos[i] == gs.nos[i];
       if (!same) continue;
       if (fg.first_slice < 0) fg.first_slice = s;
-      const SliceGeom& g0 = P->h_slices[fg.first_slice];
+      const SliceGeom& g0 = hsl[fg.first_slice];
       for (int i = 0; i < D; ++i) fg.native &= g.n[i] == g0.n[i];
       sl_ids.push_back(s);
       rows.push_back(r);
@@ -539,18 +590,19 @@ int ffx_setup(mrn_plan* P) {
     }
     rows.push_back(r);
     fg.nrows = r;
+    if (fg.first_slice < 0) fg.native = false;
     for (int i = 0; i < D; ++i) {
       FfxAxis& ax = fg.ax[i];
-      if (!ffx_factor(P->fft[q].nos[i], ax)) {
+      if (!ffx_factor(gs.nos[i], ax)) {
         fg.native = false;
         continue;
       }
       ax.tw_base = (int)tab.size();
       int L = 1, off = 0;
-      for (int s = 0; s < ax.ns; ++s) {
-        const int R = ax.radix[s];
-        ax.tw_off[s] = off;
-        ax.magic[s] = L > 1 ? (unsigned)((1ull << 32) / (unsigned long long)L + 1ull) : 0u;
+      for (int st = 0; st < ax.ns; ++st) {
+        const int R = ax.radix[st];
+        ax.tw_off[st] = off;
+        ax.magic[st] = L > 1 ? (unsigned)((1ull << 32) / (unsigned long long)L + 1ull) : 0u;
         for (int j = 0; j < L; ++j)
           for (int t = 1; t < R; ++t) {
             const double ang = -2.0 * M_PI * (double)t * (double)j / (double)(L * R);
@@ -561,94 +613,91 @@ int ffx_setup(mrn_plan* P) {
       }
     }
     nnative += fg.native ? 1 : 0;
-    P->ffx.push_back(fg);
+    S.grp.push_back(fg);
   }
   if (nnative == 0) {
-    P->ffx.clear();
+    S.grp.clear();
     return MRN_OK;
   }
-  int rc = upload(&P->d_ffx_tw, tab);
-  if (rc == MRN_OK) rc = upload(&P->d_ffx_sl, sl_ids);
-  if (rc == MRN_OK) rc = upload(&P->d_ffx_row, rows);
+  int rc = upload(&S.d_tw, tab);
+  if (rc == MRN_OK) rc = upload(&S.d_sl, sl_ids);
+  if (rc == MRN_OK) rc = upload(&S.d_row, rows);
+  if (rc != MRN_OK) {
+    S.release();
+    return rc;
+  }
+  S.ok = true;
+  S.all = nnative == (int)spec.size();
+  return MRN_OK;
+}
+
+int ffx_fwd(const FfxSet& S, const FfxGrid& G, PreMode mode, const float2* src, const float2* mps, float scale,
+            cudaStream_t st) {
+  for (size_t q = 0; q < S.grp.size(); ++q) {
+    if (!S.grp[q].native) continue;
+    int rc = launch_rows(S, G, (int)q, false, mode, src, mps, nullptr, scale, st);
+    for (int a = G.ndim - 2; a >= 0 && rc == MRN_OK; --a) rc = launch_cols(S, G, (int)q, a, false, st);
+    if (rc != MRN_OK) return rc;
+  }
+  return MRN_OK;
+}
+
+int ffx_inv(const FfxSet& S, const FfxGrid& G, float2* out, float scale, cudaStream_t st) {
+  for (size_t q = 0; q < S.grp.size(); ++q) {
+    if (!S.grp[q].native) continue;
+    int rc = MRN_OK;
+    for (int a = 0; a <= G.ndim - 2 && rc == MRN_OK; ++a) rc = launch_cols(S, G, (int)q, a, true, st);
+    if (rc == MRN_OK) rc = launch_rows(S, G, (int)q, true, kPrePlain, nullptr, nullptr, out, scale, st);
+    if (rc != MRN_OK) return rc;
+  }
+  return MRN_OK;
+}
+
+bool ffx_active(const mrn_plan* P) { return P->ffx.ok && P->use_ffx; }
+
+// Per-slice flags: the slice's group runs the native passes (and k_pre /
+// k_post leave it alone).
+int ffx_refresh(mrn_plan* P) {
+  if (P->h_slices.empty() || !P->d_slices) return MRN_OK;
+  const int D = P->ndim;
+  for (auto& g : P->h_slices) {
+    g.native_fft = 0;
+    if (!P->use_ffx) continue;
+    for (const auto& fg : P->ffx.grp) {
+      bool same = fg.native;
+      for (int i = 0; i < D && same; ++i) same = g.nos[i] == fg.ax[i].n;
+      if (same) g.native_fft = 1;
+    }
+  }
+  return upload_slices(P) == cudaSuccess ? MRN_OK : MRN_ERR_CUDA;
+}
+
+// The plan grid's native FFT (plan creation, after the FFT groups exist).
+int ffx_setup(mrn_plan* P) {
+  P->ffx.release();
+  if (P->flags & MRN_PLAN_RAW) return MRN_OK;
+  std::vector<FfxGroupSpec> spec;
+  for (const auto& f : P->fft) {
+    FfxGroupSpec gs{};
+    for (int i = 0; i < kMaxDim; ++i) gs.nos[i] = f.nos[i];
+    gs.grid_off = f.grid_off;
+    gs.batch = f.batch;
+    spec.push_back(gs);
+  }
+  const int rc = ffx_build(P->ffx, P->ndim, P->h_slices, spec);
   if (rc != MRN_OK) return rc;
-  P->ffx_ok = true;
-  P->ffx_all = nnative == (int)P->fft.size();
   return ffx_refresh(P);
 }
 
 // Apodize / pad (plain image or SENSE x * maps) and forward FFT of the grid.
 int ffx_forward(mrn_plan* P, PreMode mode, const float2* src, const float2* mps, float scale, cudaStream_t st) {
-  const int D = P->ndim;
-  const bool sense = mode == kPreSense;
-  for (size_t q = 0; q < P->ffx.size(); ++q) {
-    const mrn_plan::FfxGroup& fg = P->ffx[q];
-    if (!fg.native) continue;
-    const FfxAxis& ax = fg.ax[D - 1];
-    const int nw = rows_warps(ax.n);
-    const unsigned blocks = (unsigned)((fg.nrows + nw - 1) / nw);
-    const size_t smem = ((size_t)ax.n + 2 * (size_t)nw * ax.n) * sizeof(float2);
-    const int* gsl = P->d_ffx_sl + fg.sl_off;
-    const int64_t* grow = P->d_ffx_row + fg.row_off;
-    int rc = MRN_OK;
-    if (blocks > 0) {
-#define MRN_FFX_ROWS(DD, SS)                                                                       \
-  do {                                                                                             \
-    auto kern = k_ffx_rows_fwd<DD, SS>;                                                            \
-    rc = set_dynamic_smem(kern, smem);                                                             \
-    if (rc == MRN_OK)                                                                              \
-      kern<<<blocks, nw * 32, smem, st>>>(P->d_slices, gsl, grow, fg.nsl, P->d_apod, src, mps, scale, \
-                                          P->d_grid, fg.nrows, ax, P->d_ffx_tw);                   \
-  } while (0)
-      if (D == 2) { if (sense) MRN_FFX_ROWS(2, true); else MRN_FFX_ROWS(2, false); }
-      else { if (sense) MRN_FFX_ROWS(3, true); else MRN_FFX_ROWS(3, false); }
-#undef MRN_FFX_ROWS
-      if (rc != MRN_OK) return rc;
-      cudaError_t e = cudaGetLastError();
-      if (e != cudaSuccess) return cuda_fail(e);
-    }
-    for (int a = D - 2; a >= 0; --a) {
-      rc = launch_cols(P, (int)q, a, false, st);
-      if (rc != MRN_OK) return rc;
-    }
-  }
-  return MRN_OK;
+  return ffx_fwd(P->ffx, plan_grid(P), mode, src, mps, scale, st);
 }
 
 // Inverse FFT of the grid; out != nullptr: crop / deapodize into the image
 // batch (plain adjoint), else the surviving lines stay in the grid.
 int ffx_inverse(mrn_plan* P, float2* out, float scale, cudaStream_t st) {
-  const int D = P->ndim;
-  for (size_t q = 0; q < P->ffx.size(); ++q) {
-    const mrn_plan::FfxGroup& fg = P->ffx[q];
-    if (!fg.native) continue;
-    int rc = MRN_OK;
-    for (int a = 0; a <= D - 2; ++a) {
-      rc = launch_cols(P, (int)q, a, true, st);
-      if (rc != MRN_OK) return rc;
-    }
-    const FfxAxis& ax = fg.ax[D - 1];
-    const int nw = rows_warps(ax.n);
-    const unsigned blocks = (unsigned)((fg.nrows + nw - 1) / nw);
-    if (blocks == 0) continue;
-    const size_t smem = ((size_t)ax.n + 2 * (size_t)nw * ax.n) * sizeof(float2);
-    const int* gsl = P->d_ffx_sl + fg.sl_off;
-    const int64_t* grow = P->d_ffx_row + fg.row_off;
-#define MRN_FFX_IROWS(DD, PP)                                                                      \
-  do {                                                                                             \
-    auto kern = k_ffx_rows_inv<DD, PP>;                                                            \
-    rc = set_dynamic_smem(kern, smem);                                                             \
-    if (rc == MRN_OK)                                                                              \
-      kern<<<blocks, nw * 32, smem, st>>>(P->d_slices, gsl, grow, fg.nsl, P->d_apod, P->d_grid, scale, \
-                                          out, fg.nrows, ax, P->d_ffx_tw);                         \
-  } while (0)
-    if (D == 2) { if (out) MRN_FFX_IROWS(2, true); else MRN_FFX_IROWS(2, false); }
-    else { if (out) MRN_FFX_IROWS(3, true); else MRN_FFX_IROWS(3, false); }
-#undef MRN_FFX_IROWS
-    if (rc != MRN_OK) return rc;
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(e);
-  }
-  return MRN_OK;
+  return ffx_inv(P->ffx, plan_grid(P), out, scale, st);
 }
 
 }  // namespace mrn

@@ -104,7 +104,25 @@ int inv_transform(mrn_plan* P, float2* out, cudaStream_t st);
 // Slice table upload (plan.cu): d_slices and its shared-k-space twin.
 cudaError_t upload_slices(mrn_plan* P);
 
-// Native FFT (ffx.cu)
+// Native FFT (ffx.cu). A grid buffer of FFT groups: per group its grid size,
+// the offset of its [batch][nos...] block and its coils; FfxGrid is what the
+// passes read (host and device slice tables, apodization, the buffer).
+struct FfxGroupSpec {
+  int nos[kMaxDim];
+  int64_t grid_off;
+  int batch;
+};
+struct FfxGrid {
+  int ndim;
+  const SliceGeom* hsl;
+  const SliceGeom* dsl;
+  const float* apod;
+  float2* grid;
+};
+int ffx_build(FfxSet& S, int ndim, const std::vector<SliceGeom>& hsl, const std::vector<FfxGroupSpec>& spec);
+int ffx_fwd(const FfxSet& S, const FfxGrid& G, PreMode mode, const float2* src, const float2* mps, float scale,
+            cudaStream_t st);
+int ffx_inv(const FfxSet& S, const FfxGrid& G, float2* out, float scale, cudaStream_t st);
 int ffx_setup(mrn_plan* P);
 int ffx_refresh(mrn_plan* P);  // slice flags after MRN_OPT_NATIVE_FFT changes
 bool ffx_active(const mrn_plan* P);

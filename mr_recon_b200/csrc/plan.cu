@@ -775,6 +775,7 @@ int mrn_plan_destroy(mrn_plan* P) {
   for (auto& fg : P->fft)
     if (fg.handle) cufftDestroy(fg.handle);
   toep_free(P);
+  P->ffx.release();
   void* bufs[] = {P->d_slices, P->d_slices_kshared, P->d_apod, P->d_coord_i, P->d_perm_i, P->d_coord_g, P->d_perm_g,
                   P->d_key_a, P->d_key_b, P->d_key_is, P->d_key_g, P->d_val_a, P->d_val_b, P->d_coord_tmp,
                   P->d_entry_cnt, P->d_tile_start_i, P->d_tile_end_i, P->d_tile_start_g,
@@ -783,7 +784,7 @@ int mrn_plan_destroy(mrn_plan* P) {
                   P->d_ksp_tmp, P->d_sync, P->d_wmeta_i, P->d_wtab_i, P->d_wmeta_g,
                   P->d_wtab_g, P->d_part, P->d_items_tmp, P->d_sort_key[0], P->d_sort_key[1],
                   P->d_sort_idx[0], P->d_sort_idx[1], P->d_red, P->d_rowpart, P->d_ent_of,
-                  P->d_ksp_ent, P->d_ffx_tw, P->d_ffx_sl, P->d_ffx_row};
+                  P->d_ksp_ent};
   for (void* b : bufs)
     if (b) cudaFree(b);
   delete P;
@@ -813,7 +814,7 @@ int mrn_plan_sizes(const mrn_plan* P, int64_t* o) {
 int mrn_plan_fft_kind(const mrn_plan* P) {
   if (!P) return MRN_ERR_ARG;
   if (!ffx_active(P)) return 0;
-  return P->ffx_all ? 1 : 2;
+  return P->ffx.all ? 1 : 2;
 }
 
 int mrn_plan_stats(mrn_plan* P, int64_t* o) {
