@@ -23,7 +23,7 @@
 // Each line is a Stockham autosort FFT in shared memory: stage s with radix R
 // and L = the product of the earlier radices maps butterfly b = k L + j
 // (j < L) to out[k R L + u L + j] = sum_t x[b + t n / R] w^(t j)
-// e^(-+2 pi i t u / R), w = e^(-+2 pi i / (L R)) (radices 4, 5, 3, 2); the
+// e^(-+2 pi i t u / R), w = e^(-+2 pi i / (L R)) (radices 5, 3, 8, 4, 2); the
 // twiddles come from a table computed on the host in double precision. The
 // result is in natural order after the last stage, with no bit reversal.
 #include <algorithm>
@@ -82,6 +82,23 @@ __device__ __forceinline__ void dft(float2 (&x)[R]) {
     x[2] = csub(a0, a2);
     x[1] = cadd(a1, a3);
     x[3] = csub(a1, a3);
+  } else if constexpr (R == 8) {
+    // two 4-point DFTs of the even and odd inputs, the odd ones turned by
+    // w8^u = e^(-+i pi u / 4), u = 1, 2, 3
+    constexpr float c = 0.707106781186547524f;  // sqrt(1/2)
+    float2 e[4] = {x[0], x[2], x[4], x[6]};
+    float2 o[4] = {x[1], x[3], x[5], x[7]};
+    dft<4, INV>(e);
+    dft<4, INV>(o);
+    const float2 o1 = o[1], o3 = o[3];
+    o[1] = INV ? make_float2(c * (o1.x - o1.y), c * (o1.x + o1.y)) : make_float2(c * (o1.x + o1.y), c * (o1.y - o1.x));
+    o[2] = rot<INV>(o[2], 1.0f);
+    o[3] = INV ? make_float2(c * (-o3.x - o3.y), c * (o3.x - o3.y)) : make_float2(c * (o3.y - o3.x), c * (-o3.x - o3.y));
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      x[u] = cadd(e[u], o[u]);
+      x[u + 4] = csub(e[u], o[u]);
+    }
   } else {  // R == 5
     const float2 a1 = cadd(x[1], x[4]), b1 = csub(x[1], x[4]);
     const float2 a2 = cadd(x[2], x[3]), b2 = csub(x[2], x[3]);
@@ -161,6 +178,7 @@ __device__ __forceinline__ void cols_stage(const float2* a, float2* b, int L, un
   do {                                                       \
     if (s == 0) {                                            \
       switch (R) {                                           \
+        case 8: CALL(8, true); break;                        \
         case 4: CALL(4, true); break;                        \
         case 5: CALL(5, true); break;                        \
         case 3: CALL(3, true); break;                        \
@@ -168,6 +186,7 @@ __device__ __forceinline__ void cols_stage(const float2* a, float2* b, int L, un
       }                                                      \
     } else {                                                 \
       switch (R) {                                           \
+        case 8: CALL(8, false); break;                       \
         case 4: CALL(4, false); break;                       \
         case 5: CALL(5, false); break;                       \
         case 3: CALL(3, false); break;                       \
@@ -520,21 +539,35 @@ int launch_rows(const FfxSet& S, const FfxGrid& G, int q, bool inv, PreMode mode
   return e == cudaSuccess ? MRN_OK : cuda_fail(e);
 }
 
-// Radices for n (4 first, then 5, 3, 2); false if n has another prime factor.
+// Radices for n: the 5s and 3s first (the first stage, which has no
+// twiddles, stores R apart, and an odd R keeps those stores free of bank
+// conflicts), then the power of two as 8s and one 4 or 2; false if n has
+// another prime factor.
 bool ffx_factor(int n, FfxAxis& ax) {
   ax = FfxAxis{};
   ax.n = n;
   if (n < 2 || n > kFfxMaxN) return false;
-  int m = n, s = 0;
-  for (int r : {4, 5, 3, 2}) {
+  int m = n, s = 0, e = 0;
+  auto push = [&](int r) {
+    if (s == kFfxMaxStages) return false;
+    ax.radix[s++] = r;
+    return true;
+  };
+  for (int r : {5, 3})
     while (m % r == 0) {
-      if (s == kFfxMaxStages) return false;
-      ax.radix[s++] = r;
+      if (!push(r)) return false;
       m /= r;
     }
+  while (m % 2 == 0) {
+    ++e;
+    m /= 2;
   }
+  if (m != 1) return false;
+  for (; e >= 3; e -= 3)
+    if (!push(8)) return false;
+  if (e > 0 && !push(e == 2 ? 4 : 2)) return false;
   ax.ns = s;
-  return m == 1;
+  return true;
 }
 
 template <class T>
