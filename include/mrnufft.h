@@ -140,7 +140,7 @@ int mrn_plan_fft_kind(const mrn_plan* plan);
  * gathers; the same bits). 0 skips both; set before mrn_plan_set_traj. */
 #define MRN_OPT_ENTRY_MAJOR 11
 /* MRN_OPT_NATIVE_FFT (default 1): the FFT stage as the library's own passes
- * (one per axis, Stockham in shared memory, radices 2, 3, 4, 5, 8) with the apodize /
+ * (one per axis, Stockham in shared memory, radices 2, 3, 4, 5, 8, 16) with the apodize /
  * zero-pad folded into the first forward pass and the crop / deapodize into
  * the last adjoint pass, the zero-padded lines skipped; used when every slice
  * has the same image and grid size and every grid size is a product of 2, 3

@@ -90,7 +90,7 @@ struct EntIO {
 constexpr int kKBTerms = 32;  // terms of the I0 power series kept in KBParams
 
 // One axis of the native FFT (ffx.cu): length n = radix[0] * ... *
-// radix[ns - 1], each radix 2, 3, 4, 5 or 8; stage s reads its twiddles
+// radix[ns - 1], each radix 2, 3, 4, 5, 8 or 16; stage s reads its twiddles
 // exp(-2 pi i t j / (L R)), j < L = radix[0] * ... * radix[s - 1], 1 <= t < R,
 // at tw + tw_off[s] + j (R - 1) + t - 1 of the axis' table (n - 1 entries).
 constexpr int kFfxMaxStages = 12;

@@ -23,7 +23,7 @@
 // Each line is a Stockham autosort FFT in shared memory: stage s with radix R
 // and L = the product of the earlier radices maps butterfly b = k L + j
 // (j < L) to out[k R L + u L + j] = sum_t x[b + t n / R] w^(t j)
-// e^(-+2 pi i t u / R), w = e^(-+2 pi i / (L R)) (radices 5, 3, 8, 4, 2); the
+// e^(-+2 pi i t u / R), w = e^(-+2 pi i / (L R)) (radices 5, 3, 16, 8, 4, 2); the
 // twiddles come from a table computed on the host in double precision. The
 // result is in natural order after the last stage, with no bit reversal.
 #include <algorithm>
@@ -98,6 +98,39 @@ __device__ __forceinline__ void dft(float2 (&x)[R]) {
     for (int u = 0; u < 4; ++u) {
       x[u] = cadd(e[u], o[u]);
       x[u + 4] = csub(e[u], o[u]);
+    }
+  } else if constexpr (R == 16) {
+    // 4 x 4: 4-point DFTs of the inputs r, r + 4, r + 8, r + 12, each
+    // output u1 turned by w16^(r u1), then 4-point DFTs across r; output
+    // u1 + 4 u2
+    constexpr float c16[10] = {1.0f, 0.923879532511286756f, 0.707106781186547524f, 0.382683432365089772f, 0.0f,
+                               -0.382683432365089772f, -0.707106781186547524f, -0.923879532511286756f, -1.0f,
+                               -0.923879532511286756f};
+    constexpr float s16[10] = {0.0f, 0.382683432365089772f, 0.707106781186547524f, 0.923879532511286756f, 1.0f,
+                               0.923879532511286756f, 0.707106781186547524f, 0.382683432365089772f, 0.0f,
+                               -0.382683432365089772f};
+    float2 a[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+#pragma unroll
+      for (int m = 0; m < 4; ++m) a[r][m] = x[4 * m + r];
+      dft<4, INV>(a[r]);
+    }
+#pragma unroll
+    for (int u1 = 0; u1 < 4; ++u1) {
+      float2 col[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int k = r * u1;
+        const float2 v = a[r][u1];
+        if (k == 0) col[r] = v;
+        else if (k == 4) col[r] = rot<INV>(v, 1.0f);
+        else col[r] = INV ? make_float2(v.x * c16[k] - v.y * s16[k], v.x * s16[k] + v.y * c16[k])
+                          : make_float2(v.x * c16[k] + v.y * s16[k], v.y * c16[k] - v.x * s16[k]);
+      }
+      dft<4, INV>(col);
+#pragma unroll
+      for (int u2 = 0; u2 < 4; ++u2) x[u1 + 4 * u2] = col[u2];
     }
   } else {  // R == 5
     const float2 a1 = cadd(x[1], x[4]), b1 = csub(x[1], x[4]);
@@ -178,6 +211,7 @@ __device__ __forceinline__ void cols_stage(const float2* a, float2* b, int L, un
   do {                                                       \
     if (s == 0) {                                            \
       switch (R) {                                           \
+        case 16: CALL(16, true); break;                     \
         case 8: CALL(8, true); break;                        \
         case 4: CALL(4, true); break;                        \
         case 5: CALL(5, true); break;                        \
@@ -186,6 +220,7 @@ __device__ __forceinline__ void cols_stage(const float2* a, float2* b, int L, un
       }                                                      \
     } else {                                                 \
       switch (R) {                                           \
+        case 16: CALL(16, false); break;                     \
         case 8: CALL(8, false); break;                       \
         case 4: CALL(4, false); break;                       \
         case 5: CALL(5, false); break;                       \
@@ -541,8 +576,9 @@ int launch_rows(const FfxSet& S, const FfxGrid& G, int q, bool inv, PreMode mode
 
 // Radices for n: the 5s and 3s first (the first stage, which has no
 // twiddles, stores R apart, and an odd R keeps those stores free of bank
-// conflicts), then the power of two as 8s and one 4 or 2; false if n has
-// another prime factor.
+// conflicts), then the power of two 2^e as 8s and one 4 or 2, or as 16s and
+// one 8, 4 or 2 where that takes fewer stages; false if n has another prime
+// factor.
 bool ffx_factor(int n, FfxAxis& ax) {
   ax = FfxAxis{};
   ax.n = n;
@@ -563,9 +599,11 @@ bool ffx_factor(int n, FfxAxis& ax) {
     m /= 2;
   }
   if (m != 1) return false;
-  for (; e >= 3; e -= 3)
-    if (!push(8)) return false;
-  if (e > 0 && !push(e == 2 ? 4 : 2)) return false;
+  const int stages8 = (e + 2) / 3, stages16 = (e + 3) / 4;
+  const int big = stages16 < stages8 ? 4 : 3;  // log2 of the main radix
+  for (; e >= big; e -= big)
+    if (!push(1 << big)) return false;
+  if (e > 0 && !push(1 << e)) return false;
   ax.ns = s;
   return true;
 }
