@@ -8,7 +8,7 @@
 // 1/sqrt(prod N) and the apodization are applied in the first forward / last
 // adjoint pass with the same float products as k_pre / k_post).
 //
-// Passes. Forward: the last axis first, one warp per grid line, fused with the
+// Passes. Forward: the last axis first, a half-warp per grid line, fused with the
 // apodize / pad: a line whose outer storage indices fall in the zero padding
 // is all zero and is neither computed nor stored. Then every other axis from
 // the last-but-one to the first, a CTA per block of W adjacent columns: rows
@@ -16,7 +16,7 @@
 // (untransformed) earlier-axis index lies in the padding are skipped.
 // Adjoint: the first axis first (every row read, only the rows that survive
 // the crop stored), the middle axis on the surviving planes likewise, and
-// the last axis as a warp per surviving line fused with the crop /
+// the last axis as a half-warp per surviving line fused with the crop /
 // deapodize, or stored back in place for the SENSE coil combination, which
 // reads only surviving lines.
 //
@@ -190,11 +190,12 @@ __device__ __forceinline__ void stage_axis(FfxShared& sa, float2* tw, const FfxA
   for (int i = threadIdx.x; i < ax.n - 1; i += blockDim.x) tw[i] = twg[ax.tw_base + i];
 }
 
-// All butterflies of one stage of a line (ES = 1) by the lanes of a warp.
+// All butterflies of one stage of a line (ES = 1) by the 16 lanes of a
+// half-warp (hl: lane within the half).
 template <int R, bool INV, bool FIRST>
 __device__ __forceinline__ void line_stage(const float2* a, float2* b, int L, unsigned magic, int nr,
-                                           const float2* tw, int lane) {
-  for (int bi = lane; bi < nr; bi += 32) bfly<R, INV, 1, FIRST>(a, b, L, magic, nr, tw, bi);
+                                           const float2* tw, int hl) {
+  for (int bi = hl; bi < nr; bi += 16) bfly<R, INV, 1, FIRST>(a, b, L, magic, nr, tw, bi);
 }
 
 // One stage over W adjacent columns (elements W apart) by a CTA.
@@ -230,19 +231,22 @@ __device__ __forceinline__ void cols_stage(const float2* a, float2* b, int L, un
     }                                                        \
   } while (0)
 
-// One line of n points by one warp: a holds the input, b is scratch; returns
-// the buffer that holds the transform.
+// One line of n points by a half-warp: a holds the input, b is scratch;
+// returns the buffer that holds the transform. Both halves of the warp run
+// every stage's __syncwarp; an inactive half (no line) skips the butterflies.
 template <bool INV>
 __device__ __forceinline__ float2* line_fft(float2* a, float2* b, int n, int ns, const FfxShared& sa,
-                                            const float2* tw, int lane) {
+                                            const float2* tw, int hl, bool active) {
   int L = 1;
   for (int s = 0; s < ns; ++s) {
     const int R = sa.radix[s], nr = n / R;
     const unsigned magic = sa.magic[s];
     const float2* t = tw + sa.tw_off[s];
-#define MRN_LINE_CALL(RR, FF) line_stage<RR, INV, FF>(a, b, L, magic, nr, t, lane)
-    MRN_FFX_STAGE(MRN_LINE_CALL);
+    if (active) {
+#define MRN_LINE_CALL(RR, FF) line_stage<RR, INV, FF>(a, b, L, magic, nr, t, hl)
+      MRN_FFX_STAGE(MRN_LINE_CALL);
 #undef MRN_LINE_CALL
+    }
     __syncwarp();
     float2* tmp = a;
     a = b;
@@ -271,8 +275,45 @@ __device__ __forceinline__ bool kept(int i, int n, int nos) {
   return q < n;
 }
 
+// Geometry of group row `row` (a grid line along the last axis): slice,
+// coil, the line's storage index within the coil, the image row it carries
+// (qlin, in image rows) and the outer apodization factor; false if an outer
+// storage index lies in the zero padding (the line is zero / cropped away).
+template <int D>
+__device__ __forceinline__ bool row_geom(const SliceGeom* __restrict__ sl, const int* __restrict__ gsl,
+                                         const int64_t* __restrict__ grow, int gns, const float* __restrict__ apod,
+                                         int64_t row, int n, float scale, const SliceGeom*& gp, int& c,
+                                         int64_t& lrow, int64_t& qlin, float& aout) {
+  int k = 0;
+  row_slice(grow, gns, row, k);
+  gp = sl + gsl[k];
+  const SliceGeom& g = *gp;
+  const int64_t r = row - grow[k];
+  const int64_t outer = g.gos / n;
+  c = (int)(r / outer);
+  int64_t o = r - (int64_t)c * outer;
+  lrow = o;
+  int st[kMaxDim] = {0, 0, 0};
+  for (int i = D - 2; i >= 0; --i) {
+    st[i] = (int)(o % g.nos[i]);
+    o /= g.nos[i];
+  }
+  aout = scale * g.inv_sqrt_n;
+  qlin = 0;
+  for (int i = 0; i < D - 1; ++i) {
+    int q = st[i] + g.n[i] / 2;
+    if (q >= g.nos[i]) q -= g.nos[i];
+    if (q >= g.n[i]) return false;
+    aout *= apod[g.apod_off[i] + q];
+    qlin = qlin * g.n[i] + q;
+  }
+  return true;
+}
+
 // Forward pass over the last axis fused with the apodize / pad (k_pre's
-// products): one warp per grid row (slice, coil, outer storage index).
+// products): each half-warp takes one grid row (slice, coil, outer storage
+// index); a row whose outer index is zero padding is neither computed nor
+// stored (the next pass reads it as zero).
 template <int D, bool SENSE>
 __global__ void __launch_bounds__(kFfxThreads)
 k_ffx_rows_fwd(const SliceGeom* __restrict__ sl, const int* __restrict__ gsl, const int64_t* __restrict__ grow,
@@ -285,69 +326,55 @@ k_ffx_rows_fwd(const SliceGeom* __restrict__ sl, const int* __restrict__ gsl, co
   float2* tw = fsm;
   stage_axis(sa, tw, ax, twg);
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t row = (int64_t)blockIdx.x * nw + warp;
-  if (row >= nrows) return;
-  int k = 0;
-  row_slice(grow, gns, row, k);
-  const SliceGeom& g = sl[gsl[k]];
-  const int64_t r = row - grow[k];
-  const int64_t outer = g.gos / n;
-  const int c = (int)(r / outer);
-  int64_t o = r - (int64_t)c * outer;
-  const int64_t lrow = o;
-  float aout = scale * g.inv_sqrt_n;
-  int st[kMaxDim] = {0, 0, 0};
-  for (int i = D - 2; i >= 0; --i) {
-    st[i] = (int)(o % g.nos[i]);
-    o /= g.nos[i];
-  }
-  int64_t qlin = 0;
-  for (int i = 0; i < D - 1; ++i) {
-    int q = st[i] + g.n[i] / 2;
-    if (q >= g.nos[i]) q -= g.nos[i];
-    if (q >= g.n[i]) return;  // zero padding: the line stays zero and is never read
-    aout *= apod[g.apod_off[i] + q];
-    qlin = qlin * g.n[i] + q;
-  }
-  const int nl = g.n[D - 1], h = nl / 2;
-  qlin *= nl;
-  const float* al = apod + g.apod_off[D - 1];
-  const float2* srow = SENSE ? src + g.x_off + qlin : src + g.img_off + (int64_t)c * g.nimg + qlin;
-  const float2* mrow = SENSE ? mps + g.img_off + (int64_t)c * g.nimg + qlin : nullptr;
-  float2* A = fsm + n + warp * 2 * n;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, half = lane >> 4, hl = lane & 15;
+  const int64_t row = ((int64_t)blockIdx.x * nw + warp) * 2 + half;
+  const SliceGeom* gp = sl;
+  int c = 0;
+  int64_t lrow = 0, qlin = 0;
+  float aout = 0.f;
+  const bool active = row < nrows && row_geom<D>(sl, gsl, grow, gns, apod, row, n, scale, gp, c, lrow, qlin, aout);
+  float2* A = fsm + n + (warp * 2 + half) * 2 * n;
   float2* B = A + n;
+  const int nl = gp->n[D - 1], h = nl / 2;
+  const int64_t q0 = qlin * nl;
+  const float* al = apod + gp->apod_off[D - 1];
+  const float2* mrow = SENSE ? mps + gp->img_off + (int64_t)c * gp->nimg + q0 : nullptr;
   // the image row lands in B (the FFT's scratch) with every copy in flight
   // at once, then is apodized and placed into A
-  for (int q = lane; q < nl; q += 32) cp_async8(&B[q], srow + q);
+  if (active) {
+    const float2* srow = SENSE ? src + gp->x_off + q0 : src + gp->img_off + (int64_t)c * gp->nimg + q0;
+    for (int q = hl; q < nl; q += 16) cp_async8(&B[q], srow + q);
+  }
   cp_async_commit();
   cp_async_wait<0>();
   __syncwarp();
-  for (int j = lane; j < n; j += 32) {
-    int q = j + h;
-    if (q >= n) q -= n;
-    float2 v = make_float2(0.f, 0.f);
-    if (q < nl) {
-      float2 x = B[q];
-      if (SENSE) {
-        const float2 m = __ldg(mrow + q);
-        x = make_float2(x.x * m.x - x.y * m.y, x.x * m.y + x.y * m.x);
+  if (active)
+    for (int j = hl; j < n; j += 16) {
+      int q = j + h;
+      if (q >= n) q -= n;
+      float2 v = make_float2(0.f, 0.f);
+      if (q < nl) {
+        float2 x = B[q];
+        if (SENSE) {
+          const float2 m = __ldg(mrow + q);
+          x = make_float2(x.x * m.x - x.y * m.y, x.x * m.y + x.y * m.x);
+        }
+        const float a = aout * al[q];
+        v = make_float2(x.x * a, x.y * a);
       }
-      const float a = aout * al[q];
-      v = make_float2(x.x * a, x.y * a);
+      A[j] = v;
     }
-    A[j] = v;
-  }
   __syncwarp();
-  const float2* res = line_fft<false>(A, B, n, ax.ns, sa, tw, lane);
-  float2* dst = grid + g.grid_off + (int64_t)c * g.gos + lrow * n;
+  const float2* res = line_fft<false>(A, B, n, ax.ns, sa, tw, hl, active);
+  if (!active) return;
+  float2* dst = grid + gp->grid_off + (int64_t)c * gp->gos + lrow * n;
 #pragma unroll 4
-  for (int j = lane; j < n; j += 32) dst[j] = res[j];
+  for (int j = hl; j < n; j += 16) dst[j] = res[j];
 }
 
-// Inverse pass over the last axis of the rows that survive the crop: POST
-// crops and deapodizes into the image (k_post's products), else the row is
-// stored back for the SENSE coil combination.
+// Inverse pass over the last axis of the rows that survive the crop (a
+// half-warp per row): POST crops and deapodizes into the image (k_post's
+// products), else the row is stored back for the SENSE coil combination.
 template <int D, bool POST>
 __global__ void __launch_bounds__(kFfxThreads)
 k_ffx_rows_inv(const SliceGeom* __restrict__ sl, const int* __restrict__ gsl, const int64_t* __restrict__ grow,
@@ -359,49 +386,33 @@ k_ffx_rows_inv(const SliceGeom* __restrict__ sl, const int* __restrict__ gsl, co
   float2* tw = fsm;
   stage_axis(sa, tw, ax, twg);
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t row = (int64_t)blockIdx.x * nw + warp;
-  if (row >= nrows) return;
-  int k = 0;
-  row_slice(grow, gns, row, k);
-  const SliceGeom& g = sl[gsl[k]];
-  const int64_t r = row - grow[k];
-  const int64_t outer = g.gos / n;
-  const int c = (int)(r / outer);
-  int64_t o = r - (int64_t)c * outer;
-  const int64_t lrow = o;
-  int st[kMaxDim] = {0, 0, 0};
-  for (int i = D - 2; i >= 0; --i) {
-    st[i] = (int)(o % g.nos[i]);
-    o /= g.nos[i];
-  }
-  float aout = scale * g.inv_sqrt_n;
-  int64_t qlin = 0;
-  for (int i = 0; i < D - 1; ++i) {
-    int q = st[i] + g.n[i] / 2;
-    if (q >= g.nos[i]) q -= g.nos[i];
-    if (q >= g.n[i]) return;  // cropped away
-    aout *= apod[g.apod_off[i] + q];
-    qlin = qlin * g.n[i] + q;
-  }
-  float2* gline = grid + g.grid_off + (int64_t)c * g.gos + lrow * n;
-  float2* A = fsm + n + warp * 2 * n;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, half = lane >> 4, hl = lane & 15;
+  const int64_t row = ((int64_t)blockIdx.x * nw + warp) * 2 + half;
+  const SliceGeom* gp = sl;
+  int c = 0;
+  int64_t lrow = 0, qlin = 0;
+  float aout = 0.f;
+  const bool active = row < nrows && row_geom<D>(sl, gsl, grow, gns, apod, row, n, scale, gp, c, lrow, qlin, aout);
+  float2* gline = grid + gp->grid_off + (int64_t)c * gp->gos + lrow * n;
+  float2* A = fsm + n + (warp * 2 + half) * 2 * n;
   float2* B = A + n;
-  for (int j = lane; j < n; j += 32) cp_async8(&A[j], gline + j);
+  if (active)
+    for (int j = hl; j < n; j += 16) cp_async8(&A[j], gline + j);
   cp_async_commit();
   cp_async_wait<0>();
   __syncwarp();
-  const float2* res = line_fft<true>(A, B, n, ax.ns, sa, tw, lane);
+  const float2* res = line_fft<true>(A, B, n, ax.ns, sa, tw, hl, active);
+  if (!active) return;
   if (!POST) {
 #pragma unroll 4
-    for (int j = lane; j < n; j += 32) gline[j] = res[j];
+    for (int j = hl; j < n; j += 16) gline[j] = res[j];
     return;
   }
-  const int nl = g.n[D - 1], h = nl / 2;
-  const float* al = apod + g.apod_off[D - 1];
-  float2* orow = out + g.img_off + (int64_t)c * g.nimg + qlin * nl;
+  const int nl = gp->n[D - 1], h = nl / 2;
+  const float* al = apod + gp->apod_off[D - 1];
+  float2* orow = out + gp->img_off + (int64_t)c * gp->nimg + qlin * nl;
 #pragma unroll 4
-  for (int j = lane; j < nl; j += 32) {
+  for (int j = hl; j < nl; j += 16) {
     int sj = j - h;
     if (sj < 0) sj += n;
     const float2 y = res[sj];
@@ -479,8 +490,9 @@ k_ffx_cols(float2* __restrict__ grid, FfxAxis ax, const float2* __restrict__ twg
 }
 
 int rows_warps(int n) {
-  // twiddles + two buffers of n points per warp within 48 KB
-  const int w = (int)((48 * 1024 / sizeof(float2) - n) / (2 * n));
+  // twiddles + two lines (a half-warp each) of two buffers of n points per
+  // warp within 48 KB
+  const int w = (int)((48 * 1024 / sizeof(float2) - n) / (4 * n));
   return std::max(1, std::min(8, w));
 }
 
@@ -537,9 +549,9 @@ int launch_rows(const FfxSet& S, const FfxGrid& G, int q, bool inv, PreMode mode
   const FfxGroup& fg = S.grp[q];
   const FfxAxis& ax = fg.ax[D - 1];
   const int nw = rows_warps(ax.n);
-  const unsigned blocks = (unsigned)((fg.nrows + nw - 1) / nw);
+  const unsigned blocks = (unsigned)((fg.nrows + 2 * nw - 1) / (2 * nw));
   if (blocks == 0) return MRN_OK;
-  const size_t smem = ((size_t)ax.n + 2 * (size_t)nw * ax.n) * sizeof(float2);
+  const size_t smem = ((size_t)ax.n + 4 * (size_t)nw * ax.n) * sizeof(float2);
   const int* gsl = S.d_sl + fg.sl_off;
   const int64_t* grow = S.d_row + fg.row_off;
   const bool sense = mode == kPreSense;
